@@ -1,0 +1,270 @@
+"""Host-side mirror of ICAR's ``advection`` module over the C ABI.
+
+Same public names, argument meaning and call order as
+src/physics/advection_driver.f90:
+    adv_var_request(options)        ->  which variables the scheme needs
+    adv_init(domain, options)       ->  create the device-resident domain
+    advect(domain, options, dt)     ->  one advection call, species in
+                                        adv_vars order
+plus the two domain methods that bracket it in a model step
+(src/main/time_step.f90:319-389): ``domain.apply_forcing(dt)`` and
+``domain.enforce_limits()``.
+
+Options and Domain carry only the fields the advection path reads, named as
+in options_t / domain_t.  Arrays are numpy float32 in the Fortran layout
+(see hicar_b200.synth).  After adv_init the device copy is authoritative:
+``domain.fetch(name)`` brings a field back, ``domain.mark_dirty(name)`` after
+a host-side change uploads it again before the next advect (CPU physics
+between advection calls).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+kADV_STD = 1
+kADV_MPDATA = 2
+kFLUXCOR_MONO = 1
+
+
+@dataclass
+class AdvOptions:                      # adv_options_type, opt_types.f90:119-127
+    boundary_buffer: bool = False
+    MPDATA_FCT: bool = True
+    mpdata_order: int = 2
+    flux_corr: int = 0
+    h_order: int = 1
+    v_order: int = 1
+
+
+@dataclass
+class PhysicsOptions:
+    advection: int = kADV_MPDATA
+
+
+@dataclass
+class TimeOptions:
+    RK3: bool = False
+
+
+@dataclass
+class Parameters:
+    advect_density: bool = False
+    debug: bool = False
+
+
+@dataclass
+class Options:
+    physics: PhysicsOptions = field(default_factory=PhysicsOptions)
+    adv_options: AdvOptions = field(default_factory=AdvOptions)
+    time_options: TimeOptions = field(default_factory=TimeOptions)
+    parameters: Parameters = field(default_factory=Parameters)
+    vars_to_allocate: set = field(default_factory=set)
+    vars_to_advect: list = field(default_factory=list)
+
+    def to_c(self) -> L.Opts:
+        a = self.adv_options
+        return L.Opts(int(self.physics.advection), int(bool(a.MPDATA_FCT)), int(a.mpdata_order), int(a.flux_corr),
+                      int(a.h_order), int(a.v_order), int(bool(self.time_options.RK3)),
+                      int(bool(self.parameters.advect_density)), int(bool(self.parameters.debug)),
+                      int(bool(a.boundary_buffer)))
+
+
+_METRIC_FIELDS = {
+    "u": L.F_U, "v": L.F_V, "w": L.F_W, "density": L.F_DENSITY, "jacobian": L.F_JACOBIAN,
+    "jacobian_u": L.F_JACOBIAN_U, "jacobian_v": L.F_JACOBIAN_V, "jacobian_w": L.F_JACOBIAN_W,
+    "advection_dz": L.F_ADVECTION_DZ,
+}
+
+
+class Domain:
+    """The advection-relevant part of domain_t for one image.
+
+    ``adv_vars`` maps species names ('qv', 'theta', 'qc', ...) to arrays in
+    the order they are advected (domain_obj.f90:62-89).
+    """
+
+    def __init__(self, nx: int, ny: int, nz: int, dx: float, device: int = 0,
+                 boundaries=(True, True, True, True)):
+        self.nx, self.ny, self.nz, self.dx = int(nx), int(ny), int(nz), float(dx)
+        self.ims, self.ime, self.jms, self.jme, self.kms, self.kme = 1, nx, 1, ny, 1, nz
+        self.device = device
+        self.north_boundary, self.south_boundary, self.east_boundary, self.west_boundary = boundaries
+        self.u = self.v = self.w = self.density = None
+        self.jacobian = self.jacobian_u = self.jacobian_v = self.jacobian_w = self.advection_dz = None
+        self.adv_vars: dict[str, np.ndarray] = {}
+        self.forcing: dict[str, tuple[np.ndarray, np.ndarray | None]] = {}
+        self._h = None
+        self._dirty: set[str] = set()
+
+    @classmethod
+    def from_case(cls, case, device: int = 0) -> "Domain":
+        d = cls(case.nx, case.ny, case.nz, case.dx, device=device)
+        for k in _METRIC_FIELDS:
+            setattr(d, k, np.ascontiguousarray(getattr(case, k), np.float32))
+        d.adv_vars = {k: np.ascontiguousarray(v, np.float32).copy() for k, v in case.species.items()}
+        return d
+
+    # -- handle plumbing -------------------------------------------------
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("adv_init(domain, options) has not been called")
+        return self._h
+
+    def _field_id(self, name: str) -> int:
+        if name in _METRIC_FIELDS:
+            return _METRIC_FIELDS[name]
+        if name in L.SPECIES_IDS:
+            return L.SPECIES_IDS[name]
+        if name.startswith("forcing_"):
+            return L.F_FORCING_BASE + L.SPECIES_IDS[name[8:]]
+        if name.startswith("dqdt_"):
+            return L.F_DQDT_BASE + L.SPECIES_IDS[name[5:]]
+        if name == "relax_filter":
+            return L.F_RELAX_FILTER
+        raise KeyError(name)
+
+    def _host_array(self, name: str) -> np.ndarray:
+        if name in _METRIC_FIELDS:
+            return getattr(self, name)
+        if name in self.adv_vars:
+            return self.adv_vars[name]
+        if name.startswith("forcing_"):
+            return self.forcing[name[8:]][0]
+        if name.startswith("dqdt_"):
+            return self.forcing[name[5:]][1]
+        raise KeyError(name)
+
+    def upload(self, name: str, arr: np.ndarray | None = None) -> None:
+        a = self._host_array(name) if arr is None else arr
+        a = np.ascontiguousarray(a, np.float32)
+        L.check(L.load().icar_adv_set_field(self.handle, self._field_id(name), L.f32_ptr(a), None), self.handle)
+
+    def fetch(self, name: str) -> np.ndarray:
+        """Copy a resident field back into (and return) its host array."""
+        a = self._host_array(name)
+        if not a.flags.c_contiguous:
+            a = np.ascontiguousarray(a)
+        L.check(L.load().icar_adv_get_field(self.handle, self._field_id(name), L.f32_ptr(a), None), self.handle)
+        if name in self.adv_vars:
+            self.adv_vars[name] = a
+        return a
+
+    def relax_filter(self) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), np.float32)
+        L.check(L.load().icar_adv_get_field(self.handle, L.F_RELAX_FILTER, L.f32_ptr(out), None), self.handle)
+        return out
+
+    def mark_dirty(self, name: str) -> None:
+        self._dirty.add(name)
+
+    def _flush(self) -> None:
+        for name in sorted(self._dirty):
+            self.upload(name)
+        self._dirty.clear()
+
+    def set_forcing(self, name: str, forcing_hi: np.ndarray, dqdt: np.ndarray | None = None) -> None:
+        """Boundary forcing of an advected species (forcing_hi and its dqdt)."""
+        self.forcing[name] = (np.ascontiguousarray(forcing_hi, np.float32).copy(),
+                              None if dqdt is None else np.ascontiguousarray(dqdt, np.float32).copy())
+        if self._h is not None:
+            self.upload("forcing_" + name)
+            if dqdt is not None:
+                self.upload("dqdt_" + name)
+
+    # -- domain methods used around advect ---------------------------------
+    def apply_forcing(self, dt_seconds: float) -> None:
+        self._flush()
+        L.check(L.load().icar_adv_apply_forcing(self.handle, C.c_double(dt_seconds)), self.handle)
+
+    def enforce_limits(self) -> None:
+        self._flush()
+        L.check(L.load().icar_adv_enforce_limits(self.handle), self.handle)
+
+    def sync(self) -> None:
+        L.check(L.load().icar_adv_sync(self.handle), self.handle)
+
+    def device_bytes(self) -> int:
+        b = C.c_int64(0)
+        L.check(L.load().icar_adv_device_bytes(self.handle, C.byref(b)), self.handle)
+        return int(b.value)
+
+    def use_staged_kernels(self, staged: bool = True) -> None:
+        L.check(L.load().icar_adv_set_path(self.handle, 1 if staged else 0), self.handle)
+
+    def close(self) -> None:
+        if self._h is not None:
+            L.load().icar_adv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def adv_var_request(options: Options) -> None:
+    """advection_driver.f90:46-57 -> adv_std_var_request (advect.f90:94-108)."""
+    lib = L.load()
+    alloc = (C.c_int32 * 8)()
+    adv = (C.c_int32 * 8)()
+    na, nv = C.c_int32(8), C.c_int32(8)
+    opts = options.to_c()
+    L.check(lib.icar_adv_var_request(C.byref(opts), alloc, C.byref(na), adv, C.byref(nv)))
+    options.vars_to_allocate |= {int(alloc[i]) for i in range(na.value)}
+    for i in range(nv.value):
+        if int(adv[i]) not in options.vars_to_advect:
+            options.vars_to_advect.append(int(adv[i]))
+
+
+def adv_init(domain: Domain, options: Options) -> None:
+    """advection_driver.f90:26-44: allocate the device-resident domain and
+    upload every field the path reads."""
+    lib = L.load()
+    if domain._h is not None:
+        domain.close()
+    desc = L.Desc()
+    desc.nx, desc.ny, desc.nz, desc.dx = domain.nx, domain.ny, domain.nz, domain.dx
+    names = list(domain.adv_vars)
+    if len(names) > L.MAX_SPECIES:
+        raise ValueError("too many advected species")
+    desc.n_species = len(names)
+    for i, n in enumerate(names):
+        desc.species[i] = L.SPECIES_IDS[n]
+    desc.north_boundary, desc.south_boundary = int(domain.north_boundary), int(domain.south_boundary)
+    desc.east_boundary, desc.west_boundary = int(domain.east_boundary), int(domain.west_boundary)
+    desc.device = domain.device
+    opts = options.to_c()
+    h = C.c_void_p()
+    L.check(lib.icar_adv_create(C.byref(desc), C.byref(opts), C.byref(h)))
+    domain._h = h
+    domain._options = options
+    for k in _METRIC_FIELDS:
+        if getattr(domain, k) is not None:
+            domain.upload(k)
+    for k in names:
+        domain.upload(k)
+    for k, (fh, dq) in domain.forcing.items():
+        domain.upload("forcing_" + k)
+        if dq is not None:
+            domain.upload("dqdt_" + k)
+    domain._dirty.clear()
+
+
+def advect(domain: Domain, options: Options, dt: float) -> None:
+    """advection_driver.f90:59-126: one advection call (asynchronous on the
+    device; fetch() or sync() to wait)."""
+    domain._flush()
+    L.check(L.load().icar_adv_advect(domain.handle, C.c_float(dt)), domain.handle)
+
+
+def step(domain: Domain, options: Options, dt_seconds: float, enforce_limits: bool = False) -> None:
+    """apply_forcing -> advect -> (enforce_limits), time_step.f90:319-389."""
+    domain._flush()
+    L.check(L.load().icar_adv_step(domain.handle, C.c_double(dt_seconds), int(enforce_limits)), domain.handle)

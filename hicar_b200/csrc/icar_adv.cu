@@ -1,0 +1,883 @@
+// libicar_adv: C ABI (include/icar_adv.h) over the sm_100a advection kernels.
+//
+// A handle (icar_adv_domain) is the device-resident image of one ICAR
+// domain_t: species, winds and metric fields live in HBM with a common row
+// pitch; the host only moves data on explicit set/get calls.  Work is
+// enqueued on the handle's stream; failures are returned as status codes with
+// a message, never by aborting.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/icar_adv.h"
+#include "boundary_kernels.cuh"
+#include "common.cuh"
+#include "mpdata_fused.cuh"
+#include "mpdata_kernels.cuh"
+#include "std_kernels.cuh"
+
+using icar::Geo;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+    float *p = nullptr;
+    size_t n = 0;  // elements
+};
+
+}  // namespace
+
+struct icar_adv_domain {
+    icar_adv_desc desc{};
+    icar_adv_opts opts{};
+    int hs = 2;
+    Geo g{};
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    size_t n_cell = 0, n_u = 0, n_v = 0, n_zf = 0;
+    size_t bytes = 0;
+    // resident inputs
+    DevBuf u, v, w, rho, jac, jac_u, jac_v, jac_w, dz;
+    bool have_u = false, have_v = false, have_w = false, have_rho = false, have_jac = false,
+         have_jac_u = false, have_jac_v = false, have_jac_w = false, have_dz = false;
+    std::vector<DevBuf> q;           // species, adv_vars order
+    std::vector<bool> have_q;
+    std::vector<DevBuf> forcing, dqdt;
+    DevBuf spare;                    // output buffer of the fused kernel (swapped with a species)
+    // relaxation zone
+    std::vector<float> filter_host;  // nx*ny
+    float *filter_dev = nullptr;
+    int *zone_dev = nullptr;
+    int nzone = 0;
+    // per-step Courant fluxes and staged-path scratch
+    DevBuf Um, Vm, Wm;
+    DevBuf q1, u2, v2, w2, u2l, v2l, w2l;      // MPDATA staged scratch
+    DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
+    int path = 0;  // 0 = fused MPDATA kernel when eligible, 1 = staged kernels
+    // diagnostics: launch counter and optional event timing of the species kernels
+    int64_t launches = 0;
+    int64_t timed_launches = 0;
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::string err;
+};
+
+namespace {
+
+int fail(icar_adv_t *h, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h)
+        h->err = buf;
+    else
+        g_create_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            return fail((h), e_ == cudaErrorMemoryAllocation ? ICAR_ADV_OOM : ICAR_ADV_CUDA_ERROR, \
+                        "%s failed: %s", #call, cudaGetErrorString(e_));                           \
+        }                                                                                          \
+    } while (0)
+
+bool is_species_id(int id) { return (id >= 7 && id <= 29 && id != 8); }
+
+int halo_for(const icar_adv_opts &o)
+{
+    // read_domain_shape, src/objects/domain_obj.f90:2979-2986, and
+    // set_grid_dimensions, src/objects/grid_obj.f90:153-154.
+    int adv_order = std::max(o.h_order, o.v_order);
+    if (o.flux_corr == ICAR_FLUXCOR_MONO) adv_order += 2;
+    if (o.advection == ICAR_ADV_MPDATA) adv_order = 4;
+    return (adv_order + 1) / 2;  // ceiling(adv_order/2.0)
+}
+
+int validate(const icar_adv_desc *d, const icar_adv_opts *o, std::string &why)
+{
+    char b[256];
+    if (!d || !o) { why = "desc/opts is NULL"; return ICAR_ADV_BAD_ARG; }
+    if (d->nx < 3 || d->ny < 3 || d->nz < 3) {
+        snprintf(b, sizeof b, "domain %dx%dx%d too small (each extent must be >= 3)", d->nx, d->ny, d->nz);
+        why = b; return ICAR_ADV_BAD_ARG;
+    }
+    if ((int64_t)d->nx * d->ny * d->nz > (int64_t)1 << 31) { why = "domain larger than 2^31 cells"; return ICAR_ADV_BAD_ARG; }
+    if (!(d->dx > 0.0f) || !std::isfinite(d->dx)) { why = "dx must be positive"; return ICAR_ADV_BAD_ARG; }
+    if (d->n_species < 0 || d->n_species > ICAR_ADV_MAX_SPECIES) { why = "n_species out of range"; return ICAR_ADV_BAD_ARG; }
+    for (int s = 0; s < d->n_species; s++) {
+        if (!is_species_id(d->species[s])) {
+            snprintf(b, sizeof b, "species[%d]=%d is not an advectable kVARS id", s, d->species[s]);
+            why = b; return ICAR_ADV_BAD_ARG;
+        }
+        for (int t = 0; t < s; t++)
+            if (d->species[t] == d->species[s]) { why = "duplicate species id"; return ICAR_ADV_BAD_ARG; }
+    }
+    if (o->advection != ICAR_ADV_STD && o->advection != ICAR_ADV_MPDATA) { why = "advection must be 1 (STD) or 2 (MPDATA)"; return ICAR_ADV_BAD_ARG; }
+    if (o->advection == ICAR_ADV_MPDATA && (o->mpdata_order < 1 || o->mpdata_order > 8)) { why = "mpdata_order must be 1..8"; return ICAR_ADV_BAD_ARG; }
+    if (o->advection == ICAR_ADV_STD) {
+        auto ok = [](int v) { return v == 1 || v == 3 || v == 5; };
+        if (!ok(o->h_order) || !ok(o->v_order)) { why = "h_order and v_order must be 1, 3 or 5"; return ICAR_ADV_BAD_ARG; }
+        if (o->flux_corr != 0 && o->flux_corr != 1) { why = "flux_corr must be 0 or 1"; return ICAR_ADV_BAD_ARG; }
+        int hs = halo_for(*o);
+        int need = 2 * hs + 1;
+        if (d->nx < need || d->ny < need) { why = "domain smaller than twice the halo"; return ICAR_ADV_BAD_ARG; }
+        int reach = o->h_order == 5 ? 3 : (o->h_order == 3 ? 2 : 1);
+        if (o->flux_corr) reach += 1;
+        if (reach > hs) { why = "stencil reaches past the halo"; return ICAR_ADV_BAD_ARG; }
+    }
+    return ICAR_ADV_OK;
+}
+
+void geometry(const icar_adv_desc &d, Geo &g, size_t &n_cell, size_t &n_u, size_t &n_v, size_t &n_zf)
+{
+    g.nx = d.nx; g.ny = d.ny; g.nz = d.nz;
+    g.P = ((d.nx + 1) + 3) / 4 * 4;
+    n_cell = (size_t)g.P * g.nz * g.ny;
+    n_u = n_cell;
+    n_v = (size_t)g.P * g.nz * (g.ny + 1);
+    n_zf = (size_t)g.P * (g.nz + 1) * g.ny;
+}
+
+// Device bytes a handle allocates (create + the lazily allocated scratch).
+int64_t footprint_bytes(const icar_adv_desc &d, const icar_adv_opts &o)
+{
+    Geo g; size_t nc, nu, nv, nzf;
+    geometry(d, g, nc, nu, nv, nzf);
+    int64_t f = 4;
+    int64_t total = 0;
+    total += f * (int64_t)(nu + nv + nc + nc * 2 + nu + nv + nc * 2);  // u v w rho jac ju jv jw dz
+    total += f * (int64_t)nc * (d.n_species + 1);                      // species + spare
+    total += f * (int64_t)(nu + nv + nc);                              // Um Vm Wm
+    if (o.advection == ICAR_ADV_MPDATA)
+        total += f * (int64_t)(nc + 2 * (nu + nv + nc));               // staged scratch
+    else
+        total += f * (int64_t)(2 * (nu + nv + nzf) + 4 * nc);
+    total += f * (int64_t)d.nx * d.ny + 4 * (int64_t)d.nx * d.ny;
+    return total;
+}
+
+int alloc(icar_adv_t *h, DevBuf &b, size_t n)
+{
+    if (b.p) return ICAR_ADV_OK;
+    cudaError_t e = cudaMalloc(&b.p, n * sizeof(float));
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return fail(h, ICAR_ADV_OOM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(float), cudaGetErrorString(e));
+    }
+    b.n = n;
+    h->bytes += n * sizeof(float);
+    e = cudaMemsetAsync(b.p, 0, n * sizeof(float), h->stream);
+    if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    return ICAR_ADV_OK;
+}
+
+void release(DevBuf &b)
+{
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.n = 0;
+}
+
+// Host mirror of init_relax_filters (src/objects/domain_obj.f90:3285-3400).
+void relax_filter(int nx, int ny, int hs, int north, int south, int east, int west, std::vector<float> &f)
+{
+    const float rs[7] = {0.9f, 0.75f, 0.6f, 0.5f, 0.4f, 0.25f, 0.1f};
+    const float rs_r[7] = {0.1f, 0.25f, 0.4f, 0.5f, 0.6f, 0.75f, 0.9f};
+    const int ims = 1, ime = nx, jms = 1, jme = ny;
+    f.assign((size_t)nx * ny, 0.0f);
+    bool corner = (west || east) && (north || south);
+    int nr = std::min(7, std::min(ime - ims - hs, jme - jms - hs));
+    auto set = [&](int i, int j, float val) {
+        if (i >= 1 && i <= nx && j >= 1 && j <= ny) f[(size_t)(i - 1) + (size_t)nx * (j - 1)] = val;
+    };
+    if (!corner) {
+        if (west) {
+            for (int j = jms; j <= jme; j++) for (int i = ims; i <= ims + hs - 1; i++) set(i, j, 1.0f);
+            for (int k = jms; k <= jme; k++) for (int m = 1; m <= nr; m++) set(ims + hs + m - 1, k, rs[m - 1]);
+        } else if (east) {
+            for (int j = jms; j <= jme; j++) for (int i = ime - hs + 1; i <= ime; i++) set(i, j, 1.0f);
+            for (int k = jms; k <= jme; k++) for (int m = 1; m <= nr; m++) set(ime - hs - nr + m, k, rs_r[m - 1]);
+        } else if (north) {
+            for (int j = jme - hs - 1; j <= jme; j++) for (int i = ims; i <= ime; i++) set(i, j, 1.0f);
+            for (int k = ims; k <= ime; k++) for (int m = 1; m <= nr; m++) set(k, jme - hs - nr + m, rs_r[m - 1]);
+        } else if (south) {
+            for (int j = jms; j <= jms + hs - 1; j++) for (int i = ims; i <= ime; i++) set(i, j, 1.0f);
+            for (int k = ims; k <= ime; k++) for (int m = 1; m <= nr; m++) set(k, jms + hs + m - 1, rs[m - 1]);
+        }
+        return;
+    }
+    if (north && west) {
+        for (int j = jms; j <= jme; j++) for (int i = ims; i <= ims + hs - 1; i++) set(i, j, 1.0f);
+        for (int j = jme - hs - 1; j <= jme; j++) for (int i = ims; i <= ime; i++) set(i, j, 1.0f);
+        for (int k = jms; k <= jme - hs; k++) for (int m = 1; m <= nr; m++) set(ims + hs + m - 1, k, rs[m - 1]);
+        for (int k = ims + hs; k <= ime; k++) for (int m = 1; m <= nr; m++) set(k, jme - hs - nr + m, rs_r[m - 1]);
+        for (int i = 1; i <= nr; i++) for (int k = 1; k <= nr; k++) set(ims + hs + i - 1, jme - hs - k + 1, rs[std::min(i, k) - 1]);
+    } else if (north && east) {
+        for (int j = jms; j <= jme; j++) for (int i = ime - hs + 1; i <= ime; i++) set(i, j, 1.0f);
+        for (int j = jme - hs - 1; j <= jme; j++) for (int i = ims; i <= ime; i++) set(i, j, 1.0f);
+        for (int k = jms; k <= jme - hs; k++) for (int m = 1; m <= nr; m++) set(ime - hs - nr + m, k, rs_r[m - 1]);
+        for (int k = ims; k <= ime - hs; k++) for (int m = 1; m <= nr; m++) set(k, jme - hs - nr + m, rs_r[m - 1]);
+        for (int i = 1; i <= nr; i++) for (int k = 1; k <= nr; k++) set(ime - hs - i + 1, jme - hs - k + 1, rs[std::min(i, k) - 1]);
+    } else if (south && west) {
+        for (int j = jms; j <= jme; j++) for (int i = ims; i <= ims + hs - 1; i++) set(i, j, 1.0f);
+        for (int j = jms; j <= jms + hs - 1; j++) for (int i = ims; i <= ime; i++) set(i, j, 1.0f);
+        for (int k = jms + hs; k <= jme; k++) for (int m = 1; m <= nr; m++) set(ims + hs + m - 1, k, rs[m - 1]);
+        for (int k = ims + hs; k <= ime; k++) for (int m = 1; m <= nr; m++) set(k, jms + hs + m - 1, rs[m - 1]);
+        for (int i = 1; i <= nr; i++) for (int k = 1; k <= nr; k++) set(ims + hs + i - 1, jms + hs + k - 1, rs[std::min(i, k) - 1]);
+    } else if (south && east) {
+        for (int j = jms; j <= jme; j++) for (int i = ime - hs + 1; i <= ime; i++) set(i, j, 1.0f);
+        for (int j = jms; j <= jms + hs - 1; j++) for (int i = ims; i <= ime; i++) set(i, j, 1.0f);
+        for (int k = jms + hs; k <= jme; k++) for (int m = 1; m <= nr; m++) set(ime - hs - nr + m, k, rs_r[m - 1]);
+        for (int k = ims; k <= ime - hs; k++) for (int m = 1; m <= nr; m++) set(k, jms + hs + m - 1, rs[m - 1]);
+        for (int i = 1; i <= nr; i++) for (int k = 1; k <= nr; k++) set(ime - hs - i + 1, jms + hs + k - 1, rs[std::min(i, k) - 1]);
+    }
+}
+
+int upload_filter(icar_adv_t *h)
+{
+    std::vector<int> zone;
+    for (int j = 0; j < h->g.ny; j++)
+        for (int i = 0; i < h->g.nx; i++)
+            if (h->filter_host[(size_t)i + (size_t)h->g.nx * j] != 0.0f) zone.push_back(i + h->g.nx * j);
+    if (h->zone_dev) { cudaFree(h->zone_dev); h->zone_dev = nullptr; }
+    h->nzone = (int)zone.size();
+    if (!h->filter_dev) {
+        CUDA_TRY(h, cudaMalloc(&h->filter_dev, sizeof(float) * h->filter_host.size()));
+        h->bytes += sizeof(float) * h->filter_host.size();
+    }
+    CUDA_TRY(h, cudaMemcpy(h->filter_dev, h->filter_host.data(), sizeof(float) * h->filter_host.size(),
+                           cudaMemcpyHostToDevice));
+    if (h->nzone > 0) {
+        CUDA_TRY(h, cudaMalloc(&h->zone_dev, sizeof(int) * zone.size()));
+        CUDA_TRY(h, cudaMemcpy(h->zone_dev, zone.data(), sizeof(int) * zone.size(), cudaMemcpyHostToDevice));
+    }
+    return ICAR_ADV_OK;
+}
+
+// Resolve a field id to its device buffer, extents and presence flag.
+struct FieldRef {
+    DevBuf *buf = nullptr;
+    int ex = 0, ey = 0;  // x extent (nx or nx+1) and y extent (ny or ny+1)
+    int ez = 0;
+    bool *flag = nullptr;
+    int species = -1;
+    bool is_forcing = false, is_dqdt = false, is_filter = false;
+};
+
+int species_slot(const icar_adv_t *h, int id)
+{
+    for (int s = 0; s < h->desc.n_species; s++)
+        if (h->desc.species[s] == id) return s;
+    return -1;
+}
+
+int resolve(icar_adv_t *h, int field, FieldRef &r)
+{
+    const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
+    r.ez = nz;
+    switch (field) {
+    case ICAR_F_U: r = {&h->u, nx + 1, ny, nz, &h->have_u}; return ICAR_ADV_OK;
+    case ICAR_F_V: r = {&h->v, nx, ny + 1, nz, &h->have_v}; return ICAR_ADV_OK;
+    case ICAR_F_W: r = {&h->w, nx, ny, nz, &h->have_w}; return ICAR_ADV_OK;
+    case ICAR_F_DENSITY: r = {&h->rho, nx, ny, nz, &h->have_rho}; return ICAR_ADV_OK;
+    case ICAR_F_JACOBIAN: r = {&h->jac, nx, ny, nz, &h->have_jac}; return ICAR_ADV_OK;
+    case ICAR_F_JACOBIAN_U: r = {&h->jac_u, nx + 1, ny, nz, &h->have_jac_u}; return ICAR_ADV_OK;
+    case ICAR_F_JACOBIAN_V: r = {&h->jac_v, nx, ny + 1, nz, &h->have_jac_v}; return ICAR_ADV_OK;
+    case ICAR_F_JACOBIAN_W: r = {&h->jac_w, nx, ny, nz, &h->have_jac_w}; return ICAR_ADV_OK;
+    case ICAR_F_ADVECTION_DZ: r = {&h->dz, nx, ny, nz, &h->have_dz}; return ICAR_ADV_OK;
+    case ICAR_F_RELAX_FILTER: r = FieldRef{}; r.ex = nx; r.ey = ny; r.ez = 1; r.is_filter = true; return ICAR_ADV_OK;
+    default: break;
+    }
+    int base = field;
+    bool fo = false, dq = false;
+    if (field >= ICAR_F_DQDT_BASE) { base = field - ICAR_F_DQDT_BASE; dq = true; }
+    else if (field >= ICAR_F_FORCING_BASE) { base = field - ICAR_F_FORCING_BASE; fo = true; }
+    int s = species_slot(h, base);
+    if (s < 0) return fail(h, ICAR_ADV_BAD_ARG, "field id %d is not a field of this domain", field);
+    r = FieldRef{};
+    r.ex = nx; r.ey = ny; r.ez = nz; r.species = s; r.is_forcing = fo; r.is_dqdt = dq;
+    if (fo) { int e = alloc(h, h->forcing[s], h->n_cell); if (e) return e; r.buf = &h->forcing[s]; }
+    else if (dq) { int e = alloc(h, h->dqdt[s], h->n_cell); if (e) return e; r.buf = &h->dqdt[s]; }
+    else r.buf = &h->q[s];
+    return ICAR_ADV_OK;
+}
+
+int copy_field(icar_adv_t *h, int field, float *host, const int64_t *strides, bool to_device)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (!host) return fail(h, ICAR_ADV_BAD_ARG, "host pointer is NULL");
+    FieldRef r;
+    int e = resolve(h, field, r);
+    if (e) return e;
+    const int ex = r.ex, ey = r.ey, ez = r.ez;
+    int64_t sx = 1, sz = ex, sy = (int64_t)ex * ez;
+    if (strides) { sx = strides[0]; sz = strides[1]; sy = strides[2]; }
+    if (r.is_filter) {
+        if (to_device) {
+            for (int j = 0; j < ey; j++)
+                for (int i = 0; i < ex; i++) h->filter_host[(size_t)i + (size_t)ex * j] = host[i * sx + j * sy];
+            return upload_filter(h);
+        }
+        for (int j = 0; j < ey; j++)
+            for (int i = 0; i < ex; i++) host[i * sx + j * sy] = h->filter_host[(size_t)i + (size_t)ex * j];
+        return ICAR_ADV_OK;
+    }
+    if (h->opts.debug && to_device) {
+        for (int j = 0; j < ey; j++)
+            for (int k = 0; k < ez; k++)
+                for (int i = 0; i < ex; i++)
+                    if (!std::isfinite(host[i * sx + k * sz + j * sy]))
+                        return fail(h, ICAR_ADV_NAN_INPUT, "field %d has a non-finite value at (%d,%d,%d)", field, i + 1, k + 1, j + 1);
+    }
+    const size_t P = (size_t)h->g.P;
+    if (sx == 1) {
+        // rows of ex contiguous floats; rows of (k,j) are at k*sz + j*sy
+        if (sy == sz * ez) {
+            cudaError_t ce;
+            if (to_device)
+                ce = cudaMemcpy2DAsync(r.buf->p, P * 4, host, (size_t)sz * 4, (size_t)ex * 4, (size_t)ez * ey,
+                                       cudaMemcpyHostToDevice, h->stream);
+            else
+                ce = cudaMemcpy2DAsync(host, (size_t)sz * 4, r.buf->p, P * 4, (size_t)ex * 4, (size_t)ez * ey,
+                                       cudaMemcpyDeviceToHost, h->stream);
+            if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaMemcpy2DAsync: %s", cudaGetErrorString(ce));
+        } else {
+            for (int j = 0; j < ey; j++) {
+                cudaError_t ce;
+                if (to_device)
+                    ce = cudaMemcpy2DAsync(r.buf->p + P * ez * j, P * 4, host + sy * j, (size_t)sz * 4, (size_t)ex * 4,
+                                           (size_t)ez, cudaMemcpyHostToDevice, h->stream);
+                else
+                    ce = cudaMemcpy2DAsync(host + sy * j, (size_t)sz * 4, r.buf->p + P * ez * j, P * 4, (size_t)ex * 4,
+                                           (size_t)ez, cudaMemcpyDeviceToHost, h->stream);
+                if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaMemcpy2DAsync: %s", cudaGetErrorString(ce));
+            }
+        }
+    } else {
+        // general strides: pack through a host staging buffer
+        std::vector<float> stage((size_t)ex * ez * ey);
+        if (to_device) {
+            for (int j = 0; j < ey; j++)
+                for (int k = 0; k < ez; k++)
+                    for (int i = 0; i < ex; i++)
+                        stage[(size_t)i + (size_t)ex * (k + (size_t)ez * j)] = host[i * sx + k * sz + j * sy];
+            CUDA_TRY(h, cudaMemcpy2DAsync(r.buf->p, P * 4, stage.data(), (size_t)ex * 4, (size_t)ex * 4,
+                                          (size_t)ez * ey, cudaMemcpyHostToDevice, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        } else {
+            CUDA_TRY(h, cudaMemcpy2DAsync(stage.data(), (size_t)ex * 4, r.buf->p, P * 4, (size_t)ex * 4,
+                                          (size_t)ez * ey, cudaMemcpyDeviceToHost, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+            for (int j = 0; j < ey; j++)
+                for (int k = 0; k < ez; k++)
+                    for (int i = 0; i < ex; i++)
+                        host[i * sx + k * sz + j * sy] = stage[(size_t)i + (size_t)ex * (k + (size_t)ez * j)];
+        }
+    }
+    if (to_device) {
+        if (r.flag) *r.flag = true;
+        if (r.species >= 0 && !r.is_forcing && !r.is_dqdt) h->have_q[r.species] = true;
+    } else {
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
+    return ICAR_ADV_OK;
+}
+
+inline unsigned blocks_for(size_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
+
+int check_launch(icar_adv_t *h, const char *what, int n = 1)
+{
+    h->launches += n;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "launch of %s failed: %s", what, cudaGetErrorString(e));
+    return ICAR_ADV_OK;
+}
+
+int ensure_ready(icar_adv_t *h)
+{
+    const char *missing = nullptr;
+    if (!h->have_u) missing = "u";
+    else if (!h->have_v) missing = "v";
+    else if (!h->have_w) missing = "w";
+    else if (!h->have_jac) missing = "jacobian";
+    else if (!h->have_jac_u) missing = "jacobian_u";
+    else if (!h->have_jac_v) missing = "jacobian_v";
+    else if (!h->have_jac_w) missing = "jacobian_w";
+    else if (!h->have_dz) missing = "advection_dz";
+    else if (!h->have_rho && (h->opts.advection == ICAR_ADV_MPDATA || h->opts.advect_density)) missing = "density";
+    if (missing) return fail(h, ICAR_ADV_NOT_READY, "field %s was never set", missing);
+    for (int s = 0; s < h->desc.n_species; s++)
+        if (!h->have_q[s]) return fail(h, ICAR_ADV_NOT_READY, "species %d was never set", h->desc.species[s]);
+    return ICAR_ADV_OK;
+}
+
+// Courant fluxes for the step (mpdata_compute_wind or adv_std_compute_wind).
+int compute_wind(icar_adv_t *h, float dt)
+{
+    const Geo &g = h->g;
+    size_t n = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+    const float *rho = h->have_rho ? h->rho.p : h->jac.p;  // only read when advect_density
+    if (h->opts.advection == ICAR_ADV_MPDATA)
+        icar::k_mpdata_wind<<<blocks_for(n, 256), 256, 0, h->stream>>>(
+            g, h->desc.dx, dt, h->opts.advect_density, h->u.p, h->v.p, h->w.p, rho, h->jac_u.p, h->jac_v.p,
+            h->jac_w.p, h->Um.p, h->Vm.p, h->Wm.p);
+    else
+        icar::k_std_wind<<<blocks_for(n, 256), 256, 0, h->stream>>>(
+            g, h->desc.dx, dt, h->opts.advect_density, h->u.p, h->v.p, h->w.p, rho, h->jac_u.p, h->jac_v.p,
+            h->jac_w.p, h->dz.p, h->Um.p, h->Vm.p, h->Wm.p);
+    return check_launch(h, "compute_wind", 1);
+}
+
+// MPDATA with the staged kernels (any mpdata_order, FCT on or off).
+int mpdata_staged(icar_adv_t *h, int s)
+{
+    const Geo &g = h->g;
+    float *q = h->q[s].p;
+    const size_t nc = (size_t)g.nx * g.nz * g.ny;
+    const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+    const int order = h->opts.mpdata_order;
+    for (int iord = 1; iord <= order; iord++) {
+        if (iord == 1) {
+            icar::k_upwind<<<blocks_for(nc, 256), 256, 0, h->stream>>>(g, q, h->Um.p, h->Vm.p, h->Wm.p, h->rho.p,
+                                                                       h->jac.p, h->dz.p, h->q1.p);
+        } else {
+            icar::k_pseudo<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, h->q1.p, h->Um.p, h->Vm.p, h->Wm.p,
+                                                                       h->rho.p, h->jac.p, h->dz.p, h->u2.p,
+                                                                       h->v2.p, h->w2.p);
+            const float *uu = h->u2.p, *vv = h->v2.p, *ww = h->w2.p;
+            if (h->opts.mpdata_fct) {
+                icar::k_fct<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, q, h->q1.p, h->u2.p, h->v2.p, h->w2.p,
+                                                                        h->u2l.p, h->v2l.p, h->w2l.p);
+                uu = h->u2l.p; vv = h->v2l.p; ww = h->w2l.p;
+            }
+            icar::k_upwind<<<blocks_for(nc, 256), 256, 0, h->stream>>>(g, h->q1.p, uu, vv, ww, h->rho.p, h->jac.p,
+                                                                       h->dz.p, q);
+        }
+        if (iord != order) {
+            if (iord > 1)
+                if (cudaMemcpyAsync(h->q1.p, q, h->n_cell * 4, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+                    return fail(h, ICAR_ADV_CUDA_ERROR, "copy q -> q2 failed");
+        } else if (iord == 1) {
+            if (cudaMemcpyAsync(q, h->q1.p, h->n_cell * 4, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess)
+                return fail(h, ICAR_ADV_CUDA_ERROR, "copy q2 -> q failed");
+        }
+    }
+    return check_launch(h, "mpdata staged kernels", 1 + (order - 1) * (h->opts.mpdata_fct ? 3 : 2));
+}
+
+// One adv_std_advect3d call: fluxes from qf scaled by t_factor, optional WRF
+// correction against qold, update written to qout (may alias qold).
+int std_advect3d(icar_adv_t *h, const float *qf, const float *qold, float *qout, float t_factor, int flux_corr)
+{
+    const Geo &g = h->g;
+    const int hs = h->hs;
+    const int its = hs, ite = g.nx - 1 - hs, jts = hs, jte = g.ny - 1 - hs;
+    int is = its, ie = ite, js = jts, je = jte;
+    if (flux_corr == 1) { is--; ie++; js--; je++; }
+    const size_t nf = (size_t)(g.nx + 1) * (g.nz + 1) * (g.ny + 1);
+    const size_t nc = (size_t)g.nx * g.nz * g.ny;
+    const float *rho = h->have_rho ? h->rho.p : h->jac.p;
+    const int ad = h->opts.advect_density;
+    icar::k_flux3<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, h->opts.h_order, h->opts.v_order, is, ie, js, je,
+                                                              t_factor, qf, h->Um.p, h->Vm.p, h->Wm.p, h->fx.p,
+                                                              h->fy.p, h->fz.p);
+    if (flux_corr == 1) {
+        icar::k_upflux<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, 0, is, ie, js, je, qold, h->Um.p, h->Vm.p,
+                                                                   h->Wm.p, h->ufx.p, h->ufy.p, h->ufz.p);
+        icar::k_upflux_predict<<<blocks_for(nc, 256), 256, 0, h->stream>>>(g, is, ie, js, je, qold, h->ufx.p,
+                                                                           h->ufy.p, h->ufz.p, h->jac.p, rho, ad,
+                                                                           h->dz.p, h->dq.p);
+        icar::k_upflux<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, 1, is, ie, js, je, h->dq.p, h->Um.p, h->Vm.p,
+                                                                   h->Wm.p, h->ufx.p, h->ufy.p, h->ufz.p);
+        icar::k_wrf_merge<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, is, ie, js, je, h->fx.p, h->fy.p, h->fz.p,
+                                                                      h->ufx.p, h->ufy.p, h->ufz.p);
+        icar::k_wrf_cells<<<blocks_for(nc, 256), 256, 0, h->stream>>>(
+            g, is, ie, js, je, qold, h->Um.p, h->Vm.p, h->Wm.p, h->fx.p, h->fy.p, h->fz.p, h->ufx.p, h->ufy.p,
+            h->ufz.p, h->jac.p, rho, ad, h->dz.p, h->sin_.p, h->sout.p);
+        icar::k_wrf_scale<<<blocks_for(nf, 256), 256, 0, h->stream>>>(g, its, ite, jts, jte, h->fx.p, h->fy.p,
+                                                                      h->fz.p, h->ufx.p, h->ufy.p, h->ufz.p,
+                                                                      h->sin_.p, h->sout.p);
+    }
+    icar::k_std_update<<<blocks_for(nc, 256), 256, 0, h->stream>>>(g, its, ite, jts, jte, qold, h->fx.p, h->fy.p,
+                                                                   h->fz.p, h->jac.p, rho, ad, h->dz.p, qout);
+    return check_launch(h, "std kernels", flux_corr == 1 ? 8 : 2);
+}
+
+int advect_impl(icar_adv_t *h, float dt)
+{
+    int e = ensure_ready(h);
+    if (e) return e;
+    if (!(dt >= 0.0f) || !std::isfinite(dt)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite and >= 0");
+    e = compute_wind(h, dt);
+    if (e) return e;
+    const bool mp = h->opts.advection == ICAR_ADV_MPDATA;
+    if (h->opts.debug) {
+        e = icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p,
+                                h->opts.advect_density || mp);
+        if (e) return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
+    }
+    for (int s = 0; s < h->desc.n_species; s++) {
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        int64_t before = h->launches;
+        if (h->profiling) {
+            cudaEventCreate(&ev0);
+            cudaEventCreate(&ev1);
+            cudaEventRecord(ev0, h->stream);
+        }
+        if (h->opts.rk3) {
+            if (!mp) {
+                float *q = h->q[s].p;
+                if ((e = std_advect3d(h, q, q, h->temp.p, 0.333f, 0))) return e;
+                if ((e = std_advect3d(h, h->temp.p, q, h->temp.p, 0.5f, 0))) return e;
+                if ((e = std_advect3d(h, h->temp.p, q, q, 1.0f, h->opts.flux_corr))) return e;
+            }
+            // MPDATA with RK3 does nothing in the reference (advection_driver.f90:112-115)
+        } else if (!mp) {
+            float *q = h->q[s].p;
+            if ((e = std_advect3d(h, q, q, q, 1.0f, h->opts.flux_corr))) return e;
+        } else if (h->path == 0 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct)) {
+            e = icar::launch_mpdata_fused(h->stream, h->g, h->q[s].p, h->spare.p, h->Um.p, h->Vm.p, h->Wm.p,
+                                          h->rho.p, h->jac.p, h->dz.p);
+            if (e) return fail(h, ICAR_ADV_CUDA_ERROR, "fused MPDATA launch failed: %s",
+                               cudaGetErrorString(cudaGetLastError()));
+            h->launches += 1;
+            std::swap(h->q[s], h->spare);
+        } else {
+            if ((e = mpdata_staged(h, s))) return e;
+        }
+        if (h->profiling) {
+            cudaEventRecord(ev1, h->stream);
+            h->events.emplace_back(ev0, ev1);
+            h->timed_launches += h->launches - before;
+        }
+    }
+    return ICAR_ADV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int icar_adv_abi_version(void) { return ICAR_ADV_ABI_VERSION; }
+
+int icar_adv_default_opts(icar_adv_opts *o)
+{
+    if (!o) return fail(nullptr, ICAR_ADV_BAD_ARG, "opts is NULL");
+    memset(o, 0, sizeof(*o));
+    o->advection = ICAR_ADV_MPDATA;
+    o->mpdata_fct = 1;
+    o->mpdata_order = 2;
+    o->flux_corr = 0;
+    o->h_order = 1;
+    o->v_order = 1;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_var_request(const icar_adv_opts *opts, int32_t *alloc_vars, int32_t *n_alloc, int32_t *advect_vars,
+                         int32_t *n_advect)
+{
+    if (!opts || !n_alloc || !n_advect) return fail(nullptr, ICAR_ADV_BAD_ARG, "NULL argument");
+    // Both schemes request through adv_std_var_request (advection_driver.f90:52-56).
+    const int32_t alloc[5] = {ICAR_F_U, ICAR_F_V, ICAR_F_W, ICAR_F_DZ_INTERFACE, ICAR_F_QV};
+    const int32_t adv[2] = {ICAR_F_QV, ICAR_F_THETA};
+    if (*n_alloc < 5 || *n_advect < 2 || !alloc_vars || !advect_vars) {
+        *n_alloc = 5;
+        *n_advect = 2;
+        return fail(nullptr, ICAR_ADV_BAD_ARG, "output arrays need room for 5 and 2 ids");
+    }
+    memcpy(alloc_vars, alloc, sizeof alloc);
+    memcpy(advect_vars, adv, sizeof adv);
+    *n_alloc = 5;
+    *n_advect = 2;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_halo_size(const icar_adv_opts *opts)
+{
+    if (!opts) return -1;
+    return halo_for(*opts);
+}
+
+int icar_adv_footprint(const icar_adv_desc *desc, const icar_adv_opts *opts, int64_t *bytes)
+{
+    std::string why;
+    int e = validate(desc, opts, why);
+    if (e) return fail(nullptr, e, "%s", why.c_str());
+    if (!bytes) return fail(nullptr, ICAR_ADV_BAD_ARG, "bytes is NULL");
+    *bytes = footprint_bytes(*desc, *opts);
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_create(const icar_adv_desc *desc, const icar_adv_opts *opts, icar_adv_t **out)
+{
+    if (!out) return fail(nullptr, ICAR_ADV_BAD_ARG, "out is NULL");
+    *out = nullptr;
+    std::string why;
+    int e = validate(desc, opts, why);
+    if (e) return fail(nullptr, e, "%s", why.c_str());
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0)
+        return fail(nullptr, ICAR_ADV_CUDA_ERROR, "no CUDA device available: %s", cudaGetErrorString(ce));
+    if (desc->device < 0 || desc->device >= ndev) return fail(nullptr, ICAR_ADV_BAD_ARG, "device %d out of range", desc->device);
+    ce = cudaSetDevice(desc->device);
+    if (ce != cudaSuccess) return fail(nullptr, ICAR_ADV_CUDA_ERROR, "cudaSetDevice: %s", cudaGetErrorString(ce));
+
+    icar_adv_t *h = new icar_adv_domain();
+    h->desc = *desc;
+    h->opts = *opts;
+    h->hs = halo_for(*opts);
+    geometry(*desc, h->g, h->n_cell, h->n_u, h->n_v, h->n_zf);
+    ce = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        delete h;
+        return fail(nullptr, ICAR_ADV_CUDA_ERROR, "cudaStreamCreate: %s", cudaGetErrorString(ce));
+    }
+    h->stream = h->own_stream;
+    const int S = desc->n_species;
+    h->q.resize(S);
+    h->have_q.assign(S, false);
+    h->forcing.resize(S);
+    h->dqdt.resize(S);
+    auto bail = [&](int code) {
+        g_create_error = h->err;
+        icar_adv_destroy(h);
+        return code;
+    };
+    const size_t nc = h->n_cell, nu = h->n_u, nv = h->n_v;
+    if ((e = alloc(h, h->u, nu)) || (e = alloc(h, h->v, nv)) || (e = alloc(h, h->w, nc)) ||
+        (e = alloc(h, h->rho, nc)) || (e = alloc(h, h->jac, nc)) || (e = alloc(h, h->jac_u, nu)) ||
+        (e = alloc(h, h->jac_v, nv)) || (e = alloc(h, h->jac_w, nc)) || (e = alloc(h, h->dz, nc)) ||
+        (e = alloc(h, h->Um, nu)) || (e = alloc(h, h->Vm, nv)) || (e = alloc(h, h->Wm, nc)) ||
+        (e = alloc(h, h->spare, nc)))
+        return bail(e);
+    for (int s = 0; s < S; s++)
+        if ((e = alloc(h, h->q[s], nc))) return bail(e);
+    if (opts->advection == ICAR_ADV_MPDATA) {
+        if ((e = alloc(h, h->q1, nc)) || (e = alloc(h, h->u2, nu)) || (e = alloc(h, h->v2, nv)) ||
+            (e = alloc(h, h->w2, nc)) || (e = alloc(h, h->u2l, nu)) || (e = alloc(h, h->v2l, nv)) ||
+            (e = alloc(h, h->w2l, nc)))
+            return bail(e);
+    } else {
+        if ((e = alloc(h, h->fx, nu)) || (e = alloc(h, h->fy, nv)) || (e = alloc(h, h->fz, h->n_zf)) ||
+            (e = alloc(h, h->temp, nc)))
+            return bail(e);
+        if (opts->flux_corr == 1)
+            if ((e = alloc(h, h->ufx, nu)) || (e = alloc(h, h->ufy, nv)) || (e = alloc(h, h->ufz, h->n_zf)) ||
+                (e = alloc(h, h->dq, nc)) || (e = alloc(h, h->sin_, nc)) || (e = alloc(h, h->sout, nc)))
+                return bail(e);
+    }
+    relax_filter(desc->nx, desc->ny, h->hs, desc->north_boundary, desc->south_boundary, desc->east_boundary,
+                 desc->west_boundary, h->filter_host);
+    if ((e = upload_filter(h))) return bail(e);
+    ce = cudaStreamSynchronize(h->stream);
+    if (ce != cudaSuccess) {
+        h->err = std::string("initialisation failed: ") + cudaGetErrorString(ce);
+        return bail(ICAR_ADV_CUDA_ERROR);
+    }
+    *out = h;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_destroy(icar_adv_t *h)
+{
+    if (!h) return ICAR_ADV_OK;
+    cudaSetDevice(h->desc.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
+                      &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
+                      &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp})
+        release(*b);
+    for (auto &b : h->q) release(b);
+    for (auto &b : h->forcing) release(b);
+    for (auto &b : h->dqdt) release(b);
+    if (h->filter_dev) cudaFree(h->filter_dev);
+    if (h->zone_dev) cudaFree(h->zone_dev);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_set_field(icar_adv_t *h, int32_t field, const float *host, const int64_t *strides)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    return copy_field(h, field, const_cast<float *>(host), strides, true);
+}
+
+int icar_adv_get_field(icar_adv_t *h, int32_t field, float *host, const int64_t *strides)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    return copy_field(h, field, host, strides, false);
+}
+
+static int device_copy(icar_adv_t *h, int32_t field, float *dev, bool to_handle)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (!dev) return fail(h, ICAR_ADV_BAD_ARG, "device pointer is NULL");
+    cudaSetDevice(h->desc.device);
+    FieldRef r;
+    int e = resolve(h, field, r);
+    if (e) return e;
+    if (r.is_filter) return fail(h, ICAR_ADV_BAD_ARG, "the relaxation filter is set from host memory");
+    const size_t P = (size_t)h->g.P;
+    cudaError_t ce;
+    if (to_handle)
+        ce = cudaMemcpy2DAsync(r.buf->p, P * 4, dev, (size_t)r.ex * 4, (size_t)r.ex * 4, (size_t)r.ez * r.ey,
+                               cudaMemcpyDeviceToDevice, h->stream);
+    else
+        ce = cudaMemcpy2DAsync(dev, (size_t)r.ex * 4, r.buf->p, P * 4, (size_t)r.ex * 4, (size_t)r.ez * r.ey,
+                               cudaMemcpyDeviceToDevice, h->stream);
+    if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaMemcpy2DAsync: %s", cudaGetErrorString(ce));
+    if (to_handle) {
+        if (r.flag) *r.flag = true;
+        if (r.species >= 0 && !r.is_forcing && !r.is_dqdt) h->have_q[r.species] = true;
+    }
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_set_field_device(icar_adv_t *h, int32_t field, const float *dev)
+{
+    return device_copy(h, field, const_cast<float *>(dev), true);
+}
+
+int icar_adv_get_field_device(icar_adv_t *h, int32_t field, float *dev) { return device_copy(h, field, dev, false); }
+
+int icar_adv_advect(icar_adv_t *h, float dt)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    return advect_impl(h, dt);
+}
+
+int icar_adv_apply_forcing(icar_adv_t *h, double dt_seconds)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    if (!std::isfinite(dt_seconds)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite");
+    if (h->nzone == 0) return ICAR_ADV_OK;
+    const size_t n = (size_t)h->nzone * h->g.nz;
+    int launched = 0;
+    for (int s = 0; s < h->desc.n_species; s++) {
+        if (!h->forcing[s].p) continue;
+        launched++;
+        if (!h->dqdt[s].p) {
+            int e = alloc(h, h->dqdt[s], h->n_cell);  // zero tendency: fixed inflow
+            if (e) return e;
+        }
+        icar::k_apply_forcing<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->g, h->nzone, h->zone_dev, h->filter_dev,
+                                                                          dt_seconds, h->q[s].p, h->forcing[s].p,
+                                                                          h->dqdt[s].p);
+    }
+    return check_launch(h, "apply_forcing", launched);
+}
+
+int icar_adv_enforce_limits(icar_adv_t *h)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    for (int s = 0; s < h->desc.n_species; s++)
+        icar::k_enforce_limits<<<blocks_for(h->n_cell, 256), 256, 0, h->stream>>>(h->g, h->q[s].p);
+    return check_launch(h, "enforce_limits", h->desc.n_species);
+}
+
+int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits)
+{
+    int e = icar_adv_apply_forcing(h, dt_seconds);
+    if (e) return e;
+    e = icar_adv_advect(h, (float)dt_seconds);
+    if (e) return e;
+    if (enforce_limits) return icar_adv_enforce_limits(h);
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_sync(icar_adv_t *h)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "stream sync: %s", cudaGetErrorString(e));
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_set_stream(icar_adv_t *h, void *cuda_stream)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_device_bytes(const icar_adv_t *h, int64_t *bytes)
+{
+    if (!h || !bytes) return fail(nullptr, ICAR_ADV_BAD_ARG, "NULL argument");
+    *bytes = (int64_t)h->bytes;
+    return ICAR_ADV_OK;
+}
+
+const char *icar_adv_last_error(const icar_adv_t *h)
+{
+    if (!h) return g_create_error.c_str();
+    return h->err.c_str();
+}
+
+int icar_adv_profile(icar_adv_t *h, int32_t enable)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    cudaStreamSynchronize(h->stream);
+    for (auto &p : h->events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    h->events.clear();
+    h->profiling = enable != 0;
+    h->launches = 0;
+    h->timed_launches = 0;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_profile_read(icar_adv_t *h, double *species_kernel_ms, int64_t *species_kernel_launches,
+                          int64_t *all_launches, int64_t *species_passes)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    double ms = 0.0;
+    for (auto &p : h->events) {
+        float t = 0.0f;
+        CUDA_TRY(h, cudaEventElapsedTime(&t, p.first, p.second));
+        ms += t;
+    }
+    if (species_kernel_ms) *species_kernel_ms = ms;
+    if (species_kernel_launches) *species_kernel_launches = h->timed_launches;
+    if (all_launches) *all_launches = h->launches;
+    if (species_passes) *species_passes = (int64_t)h->events.size();
+    return ICAR_ADV_OK;
+}
+
+// Internal selector used by the tests and the benchmark to run the staged
+// kernels instead of the fused one (0 = fused when eligible, 1 = staged).
+int icar_adv_set_path(icar_adv_t *h, int32_t path)
+{
+    if (!h || path < 0 || path > 1) return fail(h, ICAR_ADV_BAD_ARG, "bad path");
+    h->path = path;
+    return ICAR_ADV_OK;
+}
+
+}  // extern "C"

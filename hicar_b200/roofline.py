@@ -1,0 +1,46 @@
+"""HBM roofline bookkeeping for the advection kernels.
+
+Algorithmic bytes of one MPDATA step (the bytes model): every species is
+read and written once (8 B per cell-species) and the eight species-
+independent fields (u, v, w, density, jacobian, jacobian_u/_v/_w) are read
+once per step (32 B per cell), shared by the S species:
+    8 + 32/S bytes per cell-species  (10.67 B at S=12, 40 B at S=1).
+One species pass therefore moves cells * (8 + 32/S) algorithmic bytes.
+advection_dz is one value per level and is not counted.
+"""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def bytes_per_cell_species(S: int) -> float:
+    return 8.0 + 32.0 / S
+
+
+def species_pass(nx: int, ny: int, nz: int, S: int, total_ms: float, passes: int, traffic=None) -> dict:
+    """Roofline entry for the per-species advection pass (the dominant kernel)."""
+    peak, kind = hbm_peak()
+    per_pass = nx * ny * nz * bytes_per_cell_species(S)
+    if passes <= 0 or total_ms <= 0:
+        achieved = None
+    else:
+        achieved = per_pass / (total_ms / passes / 1e3) / 1e9
+    return {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+        "peak_kind": kind, "algorithmic_bytes_per_launch": per_pass,
+        "launch_ms": (total_ms / passes) if passes else None,
+        "bytes_model": "8 + 32/S B per cell-species, one species pass per launch",
+    }

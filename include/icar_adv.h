@@ -1,0 +1,211 @@
+/*
+ * icar_adv.h -- C ABI of the B200 tracer-advection step for ICAR/HICAR.
+ *
+ * Drop-in boundary for ICAR's advection module (src/physics/advection_driver.f90,
+ * module `advection`, public :: advect, adv_init, adv_var_request).  A Fortran
+ * ISO_C_BINDING shim binds these functions one to one; plain pointers, sizes
+ * and status codes only, no C++ or CUDA types in any signature.
+ *
+ * Data model.  One handle = one ICAR image's domain (domain_t) on one GPU.
+ * Every 3-D field is passed in the Fortran layout of domain_t:
+ *   data_3d(ims:ime, kms:kme, jms:jme), x fastest, then z, then y
+ * with the staggered extents of the reference: u-grid fields (u, jacobian_u)
+ * have nx+1 points in x, v-grid fields (v, jacobian_v) have ny+1 points in y
+ * (src/objects/domain_obj.f90:1916-1931).  Host strides are given in elements
+ * for the (x, z, y) axes; {1, nx', nx'*nz} is a contiguous Fortran array.
+ * The handle owns the device copies: species, winds and metric fields stay
+ * resident in GPU memory across steps and only move on set/get calls.
+ *
+ * Errors.  Every call returns an icar_adv_status; nothing aborts.  The message
+ * of the last failure on a handle is icar_adv_last_error(h) (h may be NULL for
+ * failures that happened before a handle existed).
+ *
+ * Threading.  A handle is used by one host thread at a time; its work goes on
+ * the handle's CUDA stream.  Different handles may be driven concurrently.
+ */
+#ifndef ICAR_ADV_H
+#define ICAR_ADV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ICAR_ADV_ABI_VERSION 1
+#define ICAR_ADV_MAX_SPECIES 32
+
+/* Scheme switches, src/constants/icar_constants.f90:419-422. */
+enum { ICAR_ADV_STD = 1, ICAR_ADV_MPDATA = 2 };
+enum { ICAR_FLUXCOR_NONE = 0, ICAR_FLUXCOR_MONO = 1 };
+
+typedef enum {
+    ICAR_ADV_OK = 0,
+    ICAR_ADV_BAD_ARG = 1,        /* invalid size, id, option combination or pointer      */
+    ICAR_ADV_OOM = 2,            /* device or pinned host allocation failed              */
+    ICAR_ADV_CFL_VIOLATION = 3,  /* debug option: a Courant number >= 1 was found        */
+    ICAR_ADV_NAN_INPUT = 4,      /* debug option: a non-finite input value was found     */
+    ICAR_ADV_TIMEOUT = 5,        /* a bounded device wait gave up                        */
+    ICAR_ADV_CUDA_ERROR = 6,     /* a CUDA runtime call failed                           */
+    ICAR_ADV_NOT_READY = 7,      /* a field the step needs was never set                 */
+    ICAR_ADV_OVER_BUDGET = 8     /* admission refused: the memory budget would be exceeded */
+} icar_adv_status;
+
+/* Field ids.  Model variables use the reference's kVARS numbering
+ * (src/constants/icar_constants.f90:42-110 and the constructor at :310);
+ * domain_t members without a kVARS id use 1000+. */
+enum {
+    ICAR_F_U = 1,
+    ICAR_F_V = 2,
+    ICAR_F_W = 3,
+    ICAR_F_THETA = 7,  /* potential_temperature */
+    ICAR_F_QV = 9,     /* water_vapor */
+    ICAR_F_QC = 10,    /* cloud_water */
+    ICAR_F_NC = 11,    /* cloud_number_concentration */
+    ICAR_F_QI = 12,    /* cloud_ice */
+    ICAR_F_NI = 13,    /* ice_number_concentration */
+    ICAR_F_QR = 14,    /* rain_in_air */
+    ICAR_F_NR = 15,    /* rain_number_concentration */
+    ICAR_F_QS = 16,    /* snow_in_air */
+    ICAR_F_NS = 17,    /* snow_number_concentration */
+    ICAR_F_QG = 18,    /* graupel_in_air */
+    ICAR_F_NG = 19,    /* graupel_number_concentration */
+    ICAR_F_ICE1_A = 20, ICAR_F_ICE1_C = 21, ICAR_F_ICE2_MASS = 22, ICAR_F_ICE2_NUMBER = 23,
+    ICAR_F_ICE2_A = 24, ICAR_F_ICE2_C = 25, ICAR_F_ICE3_MASS = 26, ICAR_F_ICE3_NUMBER = 27,
+    ICAR_F_ICE3_A = 28, ICAR_F_ICE3_C = 29,
+    ICAR_F_DENSITY = 39,
+    ICAR_F_DZ_INTERFACE = 43,
+    ICAR_F_JACOBIAN = 1001,      /* domain%jacobian   (nx, nz, ny)   */
+    ICAR_F_JACOBIAN_U = 1002,    /* domain%jacobian_u (nx+1, nz, ny) */
+    ICAR_F_JACOBIAN_V = 1003,    /* domain%jacobian_v (nx, nz, ny+1) */
+    ICAR_F_JACOBIAN_W = 1004,    /* domain%jacobian_w (nx, nz, ny)   */
+    ICAR_F_ADVECTION_DZ = 1005,  /* domain%advection_dz (nx, nz, ny) */
+    ICAR_F_RELAX_FILTER = 1006,  /* domain%relax_filter_2d (nx, 1, ny); set by create, may be overridden */
+    ICAR_F_FORCING_BASE = 2000,  /* + species id: forcing_hi%data_3d of that species (nx, nz, ny) */
+    ICAR_F_DQDT_BASE = 3000      /* + species id: forcing_hi%dqdt_3d of that species  (nx, nz, ny) */
+};
+
+/* Domain description: the index bounds of one single-image domain_t
+ * (ims=jms=kms=1, ime=nx, jme=ny, kme=nz) and its advected-variable list in
+ * adv_vars order (src/objects/domain_obj.f90:62-89). */
+typedef struct {
+    int32_t nx, ny, nz;
+    float dx;                                  /* domain%dx in metres */
+    int32_t n_species;
+    int32_t species[ICAR_ADV_MAX_SPECIES];     /* kVARS ids */
+    int32_t north_boundary, south_boundary;    /* 1 where the edge is a physical boundary */
+    int32_t east_boundary, west_boundary;      /* (all four are 1 for a single image)     */
+    int32_t device;                            /* CUDA device ordinal                     */
+} icar_adv_desc;
+
+/* Options: the advection subset of options_t, field for field
+ * (adv_options_type, src/objects/opt_types.f90:119-127; physics%advection;
+ * time_options%RK3; parameters%advect_density and %debug). */
+typedef struct {
+    int32_t advection;        /* ICAR_ADV_STD or ICAR_ADV_MPDATA                 */
+    int32_t mpdata_fct;       /* MPDATA_FCT, default 1                           */
+    int32_t mpdata_order;     /* mpdata_order, default 2                         */
+    int32_t flux_corr;        /* flux_corr, default 0                            */
+    int32_t h_order;          /* h_order 1/3/5, default 1                        */
+    int32_t v_order;          /* v_order 1/3/5, default 1                        */
+    int32_t rk3;              /* time_options%RK3                                */
+    int32_t advect_density;   /* parameters%advect_density                       */
+    int32_t debug;            /* parameters%debug: NaN and Courant checks        */
+    int32_t boundary_buffer;  /* boundary_buffer (accepted; unused by the path,   */
+                              /* as in the reference)                            */
+} icar_adv_opts;
+
+typedef struct icar_adv_domain icar_adv_t;
+typedef struct icar_adv_batch icar_adv_batch_t;
+
+/* ABI version of the loaded library (ICAR_ADV_ABI_VERSION). */
+int icar_adv_abi_version(void);
+
+/* Default options, as adv_parameters_namelist sets them
+ * (src/objects/options_obj.f90:1576-1582) with physics%advection = MPDATA. */
+int icar_adv_default_opts(icar_adv_opts *opts);
+
+/* adv_var_request(options), src/physics/advection_driver.f90:46-57 ->
+ * adv_std_var_request, src/physics/advect.f90:94-108.  Writes the kVARS ids
+ * the scheme needs allocated and the ids it marks as advected; *n_* are the
+ * capacities on entry and the counts on return. */
+int icar_adv_var_request(const icar_adv_opts *opts, int32_t *alloc_vars, int32_t *n_alloc,
+                         int32_t *advect_vars, int32_t *n_advect);
+
+/* Halo width the reference derives from the options
+ * (src/objects/domain_obj.f90:2979-2986 and grid_obj.f90:153-154). */
+int icar_adv_halo_size(const icar_adv_opts *opts);
+
+/* adv_init(domain, options), src/physics/advection_driver.f90:26-44: create a
+ * handle, allocate the resident device fields, build the relaxation filter
+ * (init_relax_filters, src/objects/domain_obj.f90:3285-3400). */
+int icar_adv_create(const icar_adv_desc *desc, const icar_adv_opts *opts, icar_adv_t **out);
+int icar_adv_destroy(icar_adv_t *h);
+
+/* Copy one field between the host and the handle's resident device copy.
+ * strides: element strides of the (x, z, y) axes of the host array, or NULL
+ * for a contiguous Fortran-ordered array.  get_field returns after the data
+ * has arrived in host memory. */
+int icar_adv_set_field(icar_adv_t *h, int32_t field, const float *host, const int64_t *strides);
+int icar_adv_get_field(icar_adv_t *h, int32_t field, float *host, const int64_t *strides);
+
+/* Same with device memory on the handle's device (contiguous Fortran order).
+ * Ordered on the handle's stream. */
+int icar_adv_set_field_device(icar_adv_t *h, int32_t field, const float *dev);
+int icar_adv_get_field_device(icar_adv_t *h, int32_t field, float *dev);
+
+/* advect(domain, options, dt), src/physics/advection_driver.f90:59-126:
+ * Courant fluxes from the winds, then every species in adv_vars order.
+ * dt in seconds.  Asynchronous on the handle's stream. */
+int icar_adv_advect(icar_adv_t *h, float dt);
+
+/* apply_forcing, advected 3-D branch (src/objects/domain_obj.f90:3495-3506)
+ * for every species with a forcing field: forcing += dqdt*dt, then the
+ * relaxation-zone update.  dt_seconds is the real64 dt%seconds(). */
+int icar_adv_apply_forcing(icar_adv_t *h, double dt_seconds);
+
+/* enforce_limits (src/objects/domain_obj.f90:3124-3147): q = max(q, 0) for
+ * every resident species. */
+int icar_adv_enforce_limits(icar_adv_t *h);
+
+/* One advection time step as time_step.f90:319-389 orders it for these
+ * fields: apply_forcing(dt) -> advect(real(dt)) -> enforce_limits if
+ * enforce_limits != 0.  Asynchronous on the handle's stream. */
+int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits);
+
+/* Block until the handle's stream has drained; reports device-side errors. */
+int icar_adv_sync(icar_adv_t *h);
+
+/* Use an external CUDA stream (cudaStream_t passed as void*; NULL = the
+ * handle's own stream). */
+int icar_adv_set_stream(icar_adv_t *h, void *cuda_stream);
+
+/* Bytes of device memory the handle holds. */
+int icar_adv_device_bytes(const icar_adv_t *h, int64_t *bytes);
+
+/* Device memory a handle with this description and these options would
+ * hold, without creating it (used for admission by memory footprint). */
+int icar_adv_footprint(const icar_adv_desc *desc, const icar_adv_opts *opts, int64_t *bytes);
+
+const char *icar_adv_last_error(const icar_adv_t *h);
+
+/* Diagnostics (no reference counterpart; the reference times advect with
+ * timer_t, src/objects/timer_obj.f90).  icar_adv_profile(h, 1) resets the
+ * counters and brackets every per-species advection pass with CUDA events;
+ * icar_adv_profile_read returns the summed device time of those passes, the
+ * kernels they launched, all kernels launched since the reset and the number
+ * of passes.  Reading synchronises the handle's stream. */
+int icar_adv_profile(icar_adv_t *h, int32_t enable);
+int icar_adv_profile_read(icar_adv_t *h, double *species_kernel_ms, int64_t *species_kernel_launches,
+                          int64_t *all_launches, int64_t *species_passes);
+
+/* Kernel selection for testing: 0 = fused MPDATA kernel where it applies
+ * (default), 1 = the staged one-stage-per-kernel path. */
+int icar_adv_set_path(icar_adv_t *h, int32_t path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ICAR_ADV_H */

@@ -1,0 +1,138 @@
+"""CPU oracle: known-answer properties and golden fixtures (no GPU).
+
+The reference holds no golden vectors for the advection path; its only
+MPDATA test (src/tests/test_mpdata.f90:51-111) prints mean/min/max of a
+periodic step function.  These tests pin the restatement with that setup and
+with properties the scheme guarantees.
+"""
+import numpy as np
+import pytest
+
+from hicar_b200 import synth
+
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def _mass(case, q):
+    return float((q.astype(np.float64) * case.jacobian * case.density * case.advection_dz).sum())
+
+
+def test_reference_mpdata_periodic_step(oracle_lib):
+    """test_mpdata.f90 setup: 3x100x3, step 1->2 along y, Courant 0.25, FCT on,
+    order 2, periodic wrap after each step, 10 revolutions.  The interior mean
+    is kept to FP32 round-off and FCT keeps the field inside [1, 2]."""
+    O = oracle_lib
+    c = synth.periodic_y_case()
+    q0 = c.species["qv"]
+    nsteps = int((c.ny - 2) / 0.25) * 10
+    q = O.run_steps(c, O.make_opts(), 1.0, nsteps, wrap_y=True)["qv"]
+    m0 = q0[1:-1].mean(dtype=np.float64)
+    m1 = q[1:-1].mean(dtype=np.float64)
+    assert abs(m1 - m0) / m0 < 1e-5
+    assert q.min() >= 1.0 and q.max() <= 2.0
+
+
+def test_reference_mpdata_periodic_sine_no_fct(oracle_lib):
+    O = oracle_lib
+    c = synth.periodic_y_case(step=False)
+    q0 = c.species["qv"]
+    q = O.run_steps(c, O.make_opts(mpdata_fct=0), 1.0, int((c.ny - 2) / 0.25), wrap_y=True)["qv"]
+    assert abs(q[1:-1].mean(dtype=np.float64) - q0[1:-1].mean(dtype=np.float64)) < 1e-5
+    assert np.isfinite(q).all()
+
+
+@pytest.mark.parametrize("scheme", ["mpdata", "mpdata_nofct", "upwind", "std1", "std3", "std5", "std5_fc", "std3_rk3"])
+def test_uniform_field_invariance(oracle_lib, scheme):
+    """A uniform tracer stays uniform under the divergence-free winds."""
+    O = oracle_lib
+    c = synth.config1(nx=40, ny=36, nz=12)
+    c.species = {"qv": np.ones_like(c.species["qv"])}
+    opts = _opts(O, scheme)
+    q = O.advect(c, opts, c.dt)["qv"]
+    assert np.abs(q - 1).max() < 4e-7
+
+
+def _opts(O, scheme):
+    return {
+        "mpdata": O.make_opts(),
+        "mpdata_nofct": O.make_opts(mpdata_fct=0),
+        "upwind": O.make_opts(mpdata_order=1),
+        "std1": O.make_opts(advection=1),
+        "std3": O.make_opts(advection=1, h_order=3, v_order=3),
+        "std5": O.make_opts(advection=1, h_order=5, v_order=5),
+        "std5_fc": O.make_opts(advection=1, h_order=5, v_order=3, flux_corr=1),
+        "std3_rk3": O.make_opts(advection=1, h_order=3, v_order=3, rk3=1, flux_corr=1),
+    }[scheme]
+
+
+def test_closed_domain_mass_conservation(oracle_lib):
+    """Tracer kept away from the lateral boundaries: total mass sum(q*J*rho*dz)
+    is conserved to FP32 round-off over many steps."""
+    O = oracle_lib
+    c = synth.config1(nx=64, ny=64, nz=16)
+    y, z, x = np.meshgrid(np.arange(c.ny), np.arange(c.nz), np.arange(c.nx), indexing="ij")
+    blob = np.exp(-(((x - 24) / 5.0) ** 2 + ((y - 32) / 5.0) ** 2 + ((z - 6) / 1.5) ** 2)).astype(np.float32)
+    c.species = {"qv": blob}
+    m0 = _mass(c, blob)
+    q = O.run_steps(c, O.make_opts(), c.dt, 50)["qv"]
+    assert abs(_mass(c, q) - m0) / m0 < 2e-6
+
+
+def test_upwind_positivity(oracle_lib):
+    """Donor cell (mpdata_order 1) with Courant sum <= 1 keeps q >= 0 exactly."""
+    O = oracle_lib
+    c = synth.config2(nx=48, ny=40, nz=12)
+    c.species = {k: c.species[k] for k in ("qc", "nr")}
+    out = O.run_steps(c, O.make_opts(mpdata_order=1), c.dt, 5)
+    for q in out.values():
+        assert (q >= 0).all()
+
+
+def test_f32_tracks_f64(oracle_lib):
+    O = oracle_lib
+    c = synth.config1(nx=64, ny=48, nz=16)
+    a = O.run_steps(c, O.make_opts(), c.dt, 10)["qv"]
+    b = O.run_steps(c, O.make_opts(), c.dt, 10, dtype=np.float64)["qv"]
+    assert np.abs(a - b).max() / np.abs(b).max() < 1e-5
+
+
+def test_relax_filter_single_image(oracle_lib):
+    """Single image: all four edges physical, the north+west corner branch of
+    init_relax_filters wins, so only N and W are forced."""
+    O = oracle_lib
+    nx, ny, hs = 40, 30, 2
+    f = O.init_relax_filters(nx, ny, hs)
+    assert (f[:, :hs] == 1).all()                    # west columns
+    assert (f[ny - 2:, :] == 1).all()                # last rows stay 1
+    assert (f[: ny - hs - 7 - 1, hs + 7:] == 0).all()   # interior, south and east untouched
+    assert f[5, hs] == np.float32(0.9) and f[5, hs + 6] == np.float32(0.1)
+    assert f.max() == 1 and f.min() == 0
+
+
+def test_apply_forcing_semantics(oracle_lib):
+    O = oracle_lib
+    rng = np.random.default_rng(3)
+    ny, nz, nx = 20, 5, 24
+    q = rng.random((ny, nz, nx)).astype(np.float32)
+    fh = rng.random((ny, nz, nx)).astype(np.float32)
+    dq = (rng.random((ny, nz, nx)) * 1e-4).astype(np.float32)
+    flt = O.init_relax_filters(nx, ny, 2)
+    q1, fh1 = q.copy(), fh.copy()
+    O.apply_forcing(q1, fh1, dq, flt, 20.0)
+    fnew = (fh.astype(np.float64) + dq.astype(np.float64) * 20.0).astype(np.float32)
+    assert np.array_equal(fh1, fnew)
+    f3 = np.broadcast_to(flt[:, None, :], q.shape)
+    assert np.array_equal(q1[f3 == 1], fnew[f3 == 1])
+    relax = (q.astype(np.float64) + (f3.astype(np.float64) * 20.0 / 3600.0) * (fnew - q).astype(np.float64)).astype(np.float32)
+    m = f3 < 1
+    assert np.array_equal(q1[m], relax[m])
+
+
+def test_golden_fixtures(oracle_lib):
+    """The oracle reproduces the committed golden outputs bit for bit."""
+    from tests.golden import make_golden as G
+    for name, (case, opts, nsteps) in G.cases(oracle_lib).items():
+        ref = np.load(GOLDEN / f"{name}.npz")
+        out = oracle_lib.run_steps(case, opts, case.dt, nsteps)
+        for k, v in out.items():
+            assert np.array_equal(v, ref[k]), (name, k)
