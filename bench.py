@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--workload", default="full_species", choices=["full_species", "plain_c1"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
+    p.add_argument("--quick", action="store_true",
+                   help="timed region only (no e2e, no CPU baseline): the profiling run")
     return p.parse_args()
 
 
@@ -248,6 +250,14 @@ def run_b200(args):
     rl = roofline.species_pass(case.nx, case.ny, case.nz, S, kms.value, passes.value)
 
     # ---- end to end through the C ABI with pinned host buffers ---------
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "quick": True,
+                              "ms_per_step": ms_max / args.steps, "roofline": rl}), flush=True)
+        d.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     host = {k: torch.from_numpy(v.copy()).pin_memory() for k, v in case.species.items()}
     ids = {k: L.SPECIES_IDS[k] for k in case.species}
     e2e_steps = max(3, min(args.steps, 20))

@@ -61,6 +61,9 @@ struct icar_adv_domain {
     // per-step Courant fluxes and staged-path scratch
     DevBuf Um, Vm, Wm;
     DevBuf q1, u2, v2, w2, u2l, v2l, w2l;      // MPDATA staged scratch
+    DevBuf Gc, DJR, Wp;                        // fused path: J*rho, dz*J*rho, W_m/dz
+    std::vector<DevBuf> qn, q1s;               // fused path: next state and pass-1 result per species
+    bool fused_ready = false;
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
     int path = 0;  // 0 = fused MPDATA kernel when eligible, 1 = staged kernels
     // diagnostics: launch counter and optional event timing of the species kernels
@@ -518,20 +521,67 @@ int std_advect3d(icar_adv_t *h, const float *qf, const float *qold, float *qout,
     return check_launch(h, "std kernels", flux_corr == 1 ? 8 : 2);
 }
 
+// Fused MPDATA (order 2): prep -> pass 1 for all species -> fused
+// pseudo-velocity/FCT/corrective pass for all species, then swap buffers.
+int mpdata_fused_step(icar_adv_t *h, float dt)
+{
+    const Geo &g = h->g;
+    const int S = h->desc.n_species;
+    int e;
+    if (!h->fused_ready) {
+        h->qn.resize(S);
+        h->q1s.resize(S);
+        if ((e = alloc(h, h->Gc, h->n_cell)) || (e = alloc(h, h->DJR, h->n_cell)) || (e = alloc(h, h->Wp, h->n_cell)))
+            return e;
+        for (int s = 0; s < S; s++)
+            if ((e = alloc(h, h->qn[s], h->n_cell)) || (e = alloc(h, h->q1s[s], h->n_cell))) return e;
+        cudaError_t ce = cudaFuncSetAttribute(icar::k_mp_corr<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)icar::mpf::SMEM);
+        if (ce == cudaSuccess)
+            ce = cudaFuncSetAttribute(icar::k_mp_corr<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)icar::mpf::SMEM);
+        if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaFuncSetAttribute: %s", cudaGetErrorString(ce));
+        h->fused_ready = true;
+    }
+    const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+    icar::k_mp_prep<<<blocks_for(nf, 256), 256, 0, h->stream>>>(
+        g, h->desc.dx, dt, h->opts.advect_density, h->u.p, h->v.p, h->w.p, h->rho.p, h->jac.p, h->jac_u.p,
+        h->jac_v.p, h->jac_w.p, h->dz.p, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p, h->DJR.p, h->Wp.p);
+    if (h->opts.debug &&
+        icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p, 1))
+        return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
+    icar::SpeciesPtrs sp{};
+    for (int s = 0; s < S; s++) {
+        sp.q0[s] = h->q[s].p;
+        sp.q1[s] = h->q1s[s].p;
+        sp.out[s] = h->qn[s].p;
+    }
+    const size_t nc = (size_t)g.nx * g.nz * g.ny;
+    if (S > 0) {
+        dim3 gu(blocks_for(nc, 256), S);
+        icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p, h->DJR.p);
+        const int tx = icar::mp_tiles_x(g), ty = icar::mp_tiles_y(g);
+        const unsigned nblk = (unsigned)(tx * ty * S);
+        if (h->opts.mpdata_fct)
+            icar::k_mp_corr<true><<<nblk, icar::mpf::NT, icar::mpf::SMEM, h->stream>>>(
+                g, sp, S, tx, h->Um.p, h->Vm.p, h->Wp.p, h->Gc.p, h->DJR.p, h->dz.p);
+        else
+            icar::k_mp_corr<false><<<nblk, icar::mpf::NT, icar::mpf::SMEM, h->stream>>>(
+                g, sp, S, tx, h->Um.p, h->Vm.p, h->Wp.p, h->Gc.p, h->DJR.p, h->dz.p);
+    }
+    e = check_launch(h, "fused MPDATA kernels", S > 0 ? 3 : 1);
+    if (e) return e;
+    for (int s = 0; s < S; s++) std::swap(h->q[s], h->qn[s]);
+    return ICAR_ADV_OK;
+}
+
 int advect_impl(icar_adv_t *h, float dt)
 {
     int e = ensure_ready(h);
     if (e) return e;
     if (!(dt >= 0.0f) || !std::isfinite(dt)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite and >= 0");
-    e = compute_wind(h, dt);
-    if (e) return e;
     const bool mp = h->opts.advection == ICAR_ADV_MPDATA;
-    if (h->opts.debug) {
-        e = icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p,
-                                h->opts.advect_density || mp);
-        if (e) return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
-    }
-    for (int s = 0; s < h->desc.n_species; s++) {
+    if (mp && !h->opts.rk3 && h->path == 0 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct)) {
         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
         int64_t before = h->launches;
         if (h->profiling) {
@@ -539,6 +589,30 @@ int advect_impl(icar_adv_t *h, float dt)
             cudaEventCreate(&ev1);
             cudaEventRecord(ev0, h->stream);
         }
+        e = mpdata_fused_step(h, dt);
+        if (e) return e;
+        if (h->profiling) {
+            cudaEventRecord(ev1, h->stream);
+            h->events.emplace_back(ev0, ev1);
+            h->timed_launches += h->launches - before;
+        }
+        return ICAR_ADV_OK;
+    }
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t before = h->launches;
+    if (h->profiling) {
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, h->stream);
+    }
+    e = compute_wind(h, dt);
+    if (e) return e;
+    if (h->opts.debug) {
+        e = icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p,
+                                h->opts.advect_density || mp);
+        if (e) return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
+    }
+    for (int s = 0; s < h->desc.n_species; s++) {
         if (h->opts.rk3) {
             if (!mp) {
                 float *q = h->q[s].p;
@@ -550,21 +624,14 @@ int advect_impl(icar_adv_t *h, float dt)
         } else if (!mp) {
             float *q = h->q[s].p;
             if ((e = std_advect3d(h, q, q, q, 1.0f, h->opts.flux_corr))) return e;
-        } else if (h->path == 0 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct)) {
-            e = icar::launch_mpdata_fused(h->stream, h->g, h->q[s].p, h->spare.p, h->Um.p, h->Vm.p, h->Wm.p,
-                                          h->rho.p, h->jac.p, h->dz.p);
-            if (e) return fail(h, ICAR_ADV_CUDA_ERROR, "fused MPDATA launch failed: %s",
-                               cudaGetErrorString(cudaGetLastError()));
-            h->launches += 1;
-            std::swap(h->q[s], h->spare);
         } else {
             if ((e = mpdata_staged(h, s))) return e;
         }
-        if (h->profiling) {
-            cudaEventRecord(ev1, h->stream);
-            h->events.emplace_back(ev0, ev1);
-            h->timed_launches += h->launches - before;
-        }
+    }
+    if (h->profiling) {
+        cudaEventRecord(ev1, h->stream);
+        h->events.emplace_back(ev0, ev1);
+        h->timed_launches += h->launches - before;
     }
     return ICAR_ADV_OK;
 }
@@ -701,9 +768,16 @@ int icar_adv_destroy(icar_adv_t *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
                       &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
-                      &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp})
+                      &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp, &h->Gc,
+                      &h->DJR, &h->Wp})
         release(*b);
     for (auto &b : h->q) release(b);
+    for (auto &b : h->qn) release(b);
+    for (auto &b : h->q1s) release(b);
+    for (auto &p : h->events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
     for (auto &b : h->forcing) release(b);
     for (auto &b : h->dqdt) release(b);
     if (h->filter_dev) cudaFree(h->filter_dev);

@@ -1,5 +1,24 @@
-// Fused MPDATA step (upwind pass, pseudo-velocities, FCT limiter and the
-// corrective pass in one kernel) and the debug Courant check.
+// Fused MPDATA step for the configuration ICAR runs (mpdata_order 2, with or
+// without the FCT limiter).  Two kernels per step:
+//
+//   k_mp_prep     species-independent per-step fields: the Courant fluxes
+//                 U_m, V_m, W_m (mpdata_compute_wind) plus G = J*rho,
+//                 DJR = dz*J*rho and W' = W_m/dz, formed with exactly the
+//                 reference's operations so every later use is bit-identical.
+//   k_mp_upwind   donor-cell pass q0 -> q1 for every species in one launch;
+//                 also writes the untouched boundary ring of the output.
+//   k_mp_corr     antidiffusive pseudo-velocities, FCT limiter and the
+//                 corrective donor-cell pass, fused: one CTA owns a 28x16
+//                 column tile of one species and marches up the column,
+//                 keeping rolling z-windows of q0/q1/winds in shared memory
+//                 and the per-column z-state in registers, so every
+//                 intermediate of the reference (u2/v2/w2, the limiter's
+//                 bounds and fluxes) stays on chip.
+//
+// Reference: src/physics/adv_mpdata.f90:43-413, adv_mpdata_FCT_core.f90:47-116.
+// The limiter is applied in its per-cell form (see fct_cell_terms in
+// mpdata_kernels.cuh): each cell's in/out bounds and flux sums are computed
+// once per direction and every face reads the two cells beside it.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -7,14 +26,545 @@
 
 namespace icar {
 
-// The fused kernel covers the configuration ICAR runs: mpdata_order 2.
-inline bool fused_eligible(int order, int fct) { return false && order == 2 && fct >= 0; }
-
-inline int launch_mpdata_fused(cudaStream_t, const Geo &, const float *, float *, const float *, const float *,
-                               const float *, const float *, const float *, const float *)
+// --------------------------------------------------------------------------
+// per-step species-independent fields
+// --------------------------------------------------------------------------
+__global__ void k_mp_prep(Geo g, float dx, float dt, int adv_den, const float *__restrict__ u,
+                          const float *__restrict__ v, const float *__restrict__ w, const float *__restrict__ rho,
+                          const float *__restrict__ jac, const float *__restrict__ ju, const float *__restrict__ jv,
+                          const float *__restrict__ jw, const float *__restrict__ dz, float *__restrict__ Um,
+                          float *__restrict__ Vm, float *__restrict__ Wm, float *__restrict__ Gc,
+                          float *__restrict__ DJR, float *__restrict__ Wp)
 {
-    return 1;
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int ni = g.nx + 1, nk = g.nz, nj = g.ny + 1;
+    const int i = (int)(t % (size_t)ni);
+    size_t rest = t / (size_t)ni;
+    const int k = (int)(rest % (size_t)nk);
+    const int j = (int)(rest / (size_t)nk);
+    if (j >= nj) return;
+    if (j < g.ny) {
+        size_t c = ix(g, i, k, j);
+        if (i >= 1 && i <= g.nx - 1) {
+            float rr = adv_den ? rho[c] : 1.0f;
+            float rl = adv_den ? rho[c - 1] : 1.0f;
+            Um[c] = u[c] * dt * (rr + rl) * 0.5f * ju[c] / dx;
+        } else {
+            Um[c] = 0.0f;
+        }
+        if (i < g.nx) {
+            float r0 = adv_den ? rho[c] : 1.0f;
+            float wm;
+            if (k < g.nz - 1) {
+                float r1 = adv_den ? rho[ix(g, i, k + 1, j)] : 1.0f;
+                wm = w[c] * dt * jw[c] * (r1 + r0) * 0.5f;
+            } else {
+                wm = w[c] * dt * jw[c] * r0;
+            }
+            Wm[c] = wm;
+            const float d = dz[c], jj = jac[c], rh = rho[c];
+            Gc[c] = jj * rh;
+            DJR[c] = d * jj * rh;
+            Wp[c] = wm / d;
+        }
+    }
+    if (i < g.nx) {
+        size_t c = ix(g, i, k, j);
+        if (j >= 1 && j <= g.ny - 1) {
+            float rr = adv_den ? rho[c] : 1.0f;
+            float rl = adv_den ? rho[ix(g, i, k, j - 1)] : 1.0f;
+            Vm[c] = v[c] * dt * (rr + rl) * 0.5f * jv[c] / dx;
+        } else {
+            Vm[c] = 0.0f;
+        }
+    }
 }
+
+// Species pointer tables for the multi-species launches.
+struct SpeciesPtrs {
+    const float *q0[32];
+    float *q1[32];
+    float *out[32];
+};
+
+// --------------------------------------------------------------------------
+// donor-cell pass 1 for every species; boundary ring of `out` = q0
+// --------------------------------------------------------------------------
+__global__ void k_mp_upwind(Geo g, SpeciesPtrs sp, const float *__restrict__ U, const float *__restrict__ V,
+                            const float *__restrict__ W, const float *__restrict__ Gc,
+                            const float *__restrict__ DJR)
+{
+    const int s = blockIdx.y;
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t % (size_t)g.nx);
+    size_t rest = t / (size_t)g.nx;
+    const int k = (int)(rest % (size_t)g.nz);
+    const int j = (int)(rest / (size_t)g.nz);
+    if (j >= g.ny) return;
+    const float *__restrict__ qin = sp.q0[s];
+    const size_t c = ix(g, i, k, j);
+    const float q0 = qin[c];
+    if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) {
+        sp.q1[s][c] = q0;
+        sp.out[s][c] = q0;
+        return;
+    }
+    const size_t sy = (size_t)g.P * g.nz, sz = (size_t)g.P;
+    float fe = flux1(q0, qin[c + 1], U[c + 1]);
+    float fw = flux1(qin[c - 1], q0, U[c]);
+    float f3 = flux1(q0, qin[c + sy], V[c + sy]);
+    float f4 = flux1(qin[c - sy], q0, V[c]);
+    float val = q0 - ((fe - fw) + (f3 - f4)) / Gc[c];
+    const float djr = DJR[c];
+    if (k > 0 && k < g.nz - 1) {
+        float f5t = flux1(q0, qin[c + sz], W[c]);
+        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
+        val = val - (f5t - f5b) / djr;
+    } else if (k == 0) {
+        float f5t = flux1(q0, qin[c + sz], W[c]);
+        val = val - f5t / djr;
+    } else {
+        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
+        val = val - (q0 * W[c] - f5b) / djr;
+    }
+    sp.q1[s][c] = val;
+}
+
+namespace mpf {
+constexpr int TX = 28;            // output columns per tile
+constexpr int TY = 16;            // output rows per tile
+constexpr int PW = 32;            // plane width: x from i0-2 to i0+29
+constexpr int PH = TY + 4;        // plane height: y from j0-2 to j0+TY+1
+constexpr int PLANE = PW * PH;
+constexpr int NT = 256;
+constexpr int NW = NT / 32;
+constexpr int RPW = TY / NW;      // output rows per warp
+// shared-memory plane slots
+constexpr int S_Q1 = 0;           // 4 ring slots: level l -> S_Q1 + (l & 3)
+constexpr int S_Q0 = 4;           // 3 ring slots: level l -> S_Q0 + l % 3
+constexpr int S_U = 7;            // U_m, 3 slots
+constexpr int S_V = 10;           // V_m, 3 slots
+constexpr int S_W = 13;           // W' = W_m/dz, 3 slots
+constexpr int S_G = 16;           // G = J*rho, 3 slots
+constexpr int S_U2 = 19, S_FX = 20, S_V2 = 21, S_FY = 22;
+constexpr int S_BXI = 23, S_BXO = 24, S_BYI = 25, S_BYO = 26;
+constexpr int S_U2L = 27;         // 2 ring slots
+constexpr int S_V2L = 29;         // 2 ring slots
+constexpr int NPLANES = 31;
+constexpr size_t SMEM = (size_t)NPLANES * PLANE * sizeof(float);
+}  // namespace mpf
+
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid)
+{
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Beta of the FCT limiter, num/den with den > 0 and num >= 0.  Only
+// min(1, beta) is ever used, so a quotient >= 1 is returned as 1 without
+// dividing (num >= den implies RN(num/den) >= 1), and num == 0 gives +0
+// exactly as the division would; every other case divides.
+__device__ __forceinline__ float fct_beta(float num, float den)
+{
+    if (num >= den) return 1.0f;
+    if (num == 0.0f) return 0.0f;
+    return num / den;
+}
+
+// Asynchronously copy level `lev` of a 3-D field into a plane slot.  ex/ey
+// are the valid x/y extents of the field (nx or nx+1, ny or ny+1); cells
+// outside read as zero.
+__device__ __forceinline__ void load_plane(float *dst, const float *__restrict__ src, const Geo &g, int lev, int i0,
+                                           int j0, int ex, int ey)
+{
+    for (int e = threadIdx.x; e < mpf::PLANE; e += mpf::NT) {
+        const int lx = e % mpf::PW, ly = e / mpf::PW;
+        const int i = i0 - 2 + lx, j = j0 - 2 + ly;
+        const bool ok = i >= 0 && i < ex && j >= 0 && j < ey;
+        cp_async4(dst + e, ok ? src + ix(g, i, lev, j) : src, ok);
+    }
+}
+
+template <bool FCT>
+__global__ void __launch_bounds__(mpf::NT, 2)
+    k_mp_corr(Geo g, SpeciesPtrs sp, int nspecies, int tiles_x, const float *__restrict__ Um,
+              const float *__restrict__ Vm, const float *__restrict__ Wp, const float *__restrict__ Gc,
+              const float *__restrict__ DJR, const float *__restrict__ dz)
+{
+    using namespace mpf;
+    extern __shared__ float sm[];
+    const int s = blockIdx.x % nspecies;
+    const int tile = blockIdx.x / nspecies;
+    const int i0 = 1 + (tile % tiles_x) * TX;  // first output column (interior starts at 1)
+    const int j0 = 1 + (tile / tiles_x) * TY;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const float *__restrict__ q0g = sp.q0[s];
+    const float *__restrict__ q1g = sp.q1[s];
+    float *__restrict__ outg = sp.out[s];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float e10 = 1e-10f, e15 = 1e-15f, q4 = 1.0f / 4.0f;
+    auto P = [&](int slot) { return sm + (size_t)slot * PLANE; };
+#define AT(slot, lx, ly) sm[(size_t)(slot) * PLANE + (ly) * PW + (lx)]
+
+    // ---- prologue: levels 0 and 1 of everything the first iteration reads
+    load_plane(P(S_Q1 + 0), q1g, g, 0, i0, j0, nx, ny);
+    load_plane(P(S_Q0 + 0), q0g, g, 0, i0, j0, nx, ny);
+    load_plane(P(S_U + 0), Um, g, 0, i0, j0, nx + 1, ny);
+    load_plane(P(S_V + 0), Vm, g, 0, i0, j0, nx, ny + 1);
+    load_plane(P(S_W + 0), Wp, g, 0, i0, j0, nx, ny);
+    load_plane(P(S_G + 0), Gc, g, 0, i0, j0, nx, ny);
+    load_plane(P(S_Q1 + 1), q1g, g, 1, i0, j0, nx, ny);
+    load_plane(P(S_Q0 + 1), q0g, g, 1, i0, j0, nx, ny);
+    load_plane(P(S_U + 1), Um, g, 1, i0, j0, nx + 1, ny);
+    load_plane(P(S_V + 1), Vm, g, 1, i0, j0, nx, ny + 1);
+    load_plane(P(S_G + 1), Gc, g, 1, i0, j0, nx, ny);
+    cp_async_commit();
+
+    // per-output-cell z state (two output rows per warp)
+    // r_q1dn / r_q0dn: q1 and q0 one level below the level being limited;
+    // r_q1dd: q1 two levels below (the level under the corrective pass).
+    float r_fz[RPW], r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_w2l[RPW], r_q1dn[RPW], r_q0dn[RPW], r_q1dd[RPW];
+    float r_G[RPW], r_DJR[RPW];
+#pragma unroll
+    for (int rr = 0; rr < RPW; rr++) {
+        r_fz[rr] = r_w2[rr] = r_bzi[rr] = r_bzo[rr] = r_w2l[rr] = r_q1dn[rr] = r_q0dn[rr] = r_q1dd[rr] = 0.0f;
+        r_G[rr] = r_DJR[rr] = 1.0f;
+    }
+
+    for (int t = 0; t <= nz; t++) {
+        // planes of level t+1 (and W' of level t) must have landed
+        cp_async_wait<0>();
+        __syncthreads();
+        // prefetch the levels the next iteration adds: q1/q0/U/V/G at t+2, W' at t+1
+        if (t + 2 < nz) {
+            load_plane(P(S_Q1 + ((t + 2) & 3)), q1g, g, t + 2, i0, j0, nx, ny);
+            load_plane(P(S_Q0 + (t + 2) % 3), q0g, g, t + 2, i0, j0, nx, ny);
+            load_plane(P(S_U + (t + 2) % 3), Um, g, t + 2, i0, j0, nx + 1, ny);
+            load_plane(P(S_V + (t + 2) % 3), Vm, g, t + 2, i0, j0, nx, ny + 1);
+            load_plane(P(S_G + (t + 2) % 3), Gc, g, t + 2, i0, j0, nx, ny);
+        }
+        if (t + 1 < nz) load_plane(P(S_W + (t + 1) % 3), Wp, g, t + 1, i0, j0, nx, ny);
+        cp_async_commit();
+
+        const bool haveA = t < nz;
+        const int sQm = S_Q1 + ((t + 3) & 3), sQc = S_Q1 + (t & 3), sQp = S_Q1 + ((t + 1) & 3);
+        const int sQ0c = S_Q0 + t % 3, sQ0p = S_Q0 + (t + 1) % 3;
+        const int sUc = S_U + t % 3, sUp = S_U + (t + 1) % 3;
+        const int sVc = S_V + t % 3, sVp = S_V + (t + 1) % 3;
+        const int sWc = S_W + t % 3, sWm = S_W + (t + 2) % 3;
+        const int sGc = S_G + t % 3, sGp = S_G + (t + 1) % 3;
+        const bool kint = t > 0 && t < nz - 1;
+
+        float n_fz[RPW], n_w2[RPW], n_bzi[RPW] = {}, n_bzo[RPW] = {}, n_w2l[RPW];
+        if (haveA) {
+            // ---------------- A1: u2, v2 at level t; w2 at the top of t --------
+            for (int r = warp; r < TY; r += NW) {  // u2 faces x in [-1, TX+1] -> lx 1..31
+                const int ly = r + 2, lx = lane;
+                const int f = i0 - 2 + lx, j = j0 - 2 + ly;
+                float u2 = 0.0f, fx = 0.0f;
+                if (lx >= 1 && f >= 1 && f <= nx - 1 && j <= ny - 1) {
+                    const float rx = AT(sQc, lx, ly), lq = AT(sQc, lx - 1, ly);
+                    const float uu = AT(sUc, lx, ly);
+                    const float Gs = AT(sGc, lx, ly) + AT(sGc, lx - 1, ly);
+                    const float denom = rx + lq + e10;
+                    float val = fabsf(uu) * (1.0f - fabsf(uu) / (0.5f * Gs));
+                    val = val * (rx - lq) / denom;
+                    if (j > 0 && j < ny - 1) {
+                        const float a = AT(sQc, lx, ly + 1), b = AT(sQc, lx, ly - 1);
+                        const float c = AT(sQc, lx - 1, ly + 1), d = AT(sQc, lx - 1, ly - 1);
+                        const float eq = (a - b + c - d) / (a + b + c + d + e10);
+                        const float ev = q4 * (AT(sVc, lx, ly) + AT(sVc, lx, ly + 1) + AT(sVc, lx - 1, ly) +
+                                               AT(sVc, lx - 1, ly + 1));
+                        val = val - 0.5f * uu * ev * eq / Gs;
+                    }
+                    if (kint) {
+                        const float a = AT(sQp, lx, ly), b = AT(sQm, lx, ly);
+                        const float c = AT(sQp, lx - 1, ly), d = AT(sQm, lx - 1, ly);
+                        const float eq = (a - b + c - d) / (a + b + c + d + e10);
+                        const float ev = q4 * (AT(sWc, lx, ly) + AT(sWm, lx, ly) + AT(sWc, lx - 1, ly) +
+                                               AT(sWm, lx - 1, ly));
+                        val = val - 0.5f * uu * ev * eq / Gs;
+                    }
+                    u2 = val * 0.5f;
+                    fx = flux1(lq, rx, u2);
+                }
+                AT(S_U2, lx, ly) = u2;
+                AT(S_FX, lx, ly) = fx;
+            }
+            for (int r = warp; r < TY + 3; r += NW) {  // v2 faces y in [-1, TY+1] -> ly 1..TY+3
+                const int ly = r + 1, lx = lane;
+                const int i = i0 - 2 + lx, gf = j0 - 2 + ly;
+                float v2 = 0.0f, fy = 0.0f;
+                if (lx >= 2 && lx < TX + 2 && i <= nx - 1 && gf >= 1 && gf <= ny - 1) {
+                    const float rq = AT(sQc, lx, ly), lq = AT(sQc, lx, ly - 1);
+                    const float vv = AT(sVc, lx, ly);
+                    const float Gs = AT(sGc, lx, ly) + AT(sGc, lx, ly - 1);
+                    const float denom = rq + lq + e10;
+                    float val = fabsf(vv) * (1.0f - fabsf(vv) / (0.5f * Gs));
+                    val = val * (rq - lq) / denom;
+                    float ev = 0.0f, eq = 0.0f;
+                    if (i > 0 && i < nx - 1) {
+                        const float A = AT(sQc, lx + 1, ly - 1), B = AT(sQc, lx - 1, ly);
+                        const float C = AT(sQc, lx + 1, ly), D = AT(sQc, lx - 1, ly - 1);
+                        eq = (A - B + C - D) / (C + A + B + D + e10);
+                        ev = q4 * (AT(sUc, lx + 1, ly) + AT(sUc, lx + 1, ly - 1) + AT(sUc, lx, ly) +
+                                   AT(sUc, lx, ly - 1));
+                    }
+                    val = val - 0.5f * vv * ev * eq / Gs;
+                    if (kint) {
+                        const float A = AT(sQp, lx, ly - 1), B = AT(sQm, lx, ly);
+                        const float C = AT(sQp, lx, ly), D = AT(sQm, lx, ly - 1);
+                        const float eq2 = (A - B + C - D) / (A + B + C + D + e10);
+                        const float ev2 = q4 * (AT(sWc, lx, ly) + AT(sWm, lx, ly) + AT(sWc, lx, ly - 1) +
+                                                AT(sWm, lx, ly - 1));
+                        val = val - 0.5f * vv * ev2 * eq2 / Gs;
+                    }
+                    v2 = val * 0.5f;
+                    fy = flux1(lq, rq, v2);
+                }
+                AT(S_V2, lx, ly) = v2;
+                AT(S_FY, lx, ly) = fy;
+            }
+#pragma unroll
+            for (int rr = 0; rr < RPW; rr++) {  // w2 at the top face of level t, output cells
+                const int ly = warp + NW * rr + 2, lx = lane + 2;
+                float w2 = 0.0f, fz = 0.0f;
+                if (lane < TX && t < nz - 1) {
+                    const float rq = AT(sQp, lx, ly), lq = AT(sQc, lx, ly);
+                    const float ww = AT(sWc, lx, ly);
+                    const float Gs = AT(sGp, lx, ly) + AT(sGc, lx, ly);
+                    const float denom = rq + lq + e10;
+                    float val = fabsf(ww) * (1.0f - fabsf(ww) / (0.5f * Gs));
+                    val = val * (rq - lq) / denom;
+                    {
+                        const float A = AT(sQp, lx + 1, ly), B = AT(sQc, lx - 1, ly);
+                        const float C = AT(sQc, lx + 1, ly), D = AT(sQp, lx - 1, ly);
+                        const float eq = (A - B + C - D) / (C + A + B + D + e10);
+                        const float ev = q4 * (AT(sUc, lx + 1, ly) + AT(sUp, lx + 1, ly) + AT(sUc, lx, ly) +
+                                               AT(sUp, lx, ly));
+                        val = val - 0.5f * ww * ev * eq / Gs;
+                    }
+                    {
+                        const float A = AT(sQp, lx, ly + 1), B = AT(sQc, lx, ly - 1);
+                        const float C = AT(sQc, lx, ly + 1), D = AT(sQp, lx, ly - 1);
+                        const float eq2 = (A - B + C - D) / (C + D + A + B + e10);
+                        const float ev2 = q4 * (AT(sVc, lx, ly) + AT(sVp, lx, ly) + AT(sVc, lx, ly + 1) +
+                                                AT(sVp, lx, ly + 1));
+                        val = val - 0.5f * ww * ev2 * eq2 / Gs;
+                    }
+                    const int i = i0 - 2 + lx, j = j0 - 2 + ly;
+                    w2 = val * 0.5f * dz[ix(g, min(i, nx - 1), t, min(j, ny - 1))];
+                    fz = flux1(lq, rq, w2);
+                }
+                n_w2[rr] = w2;
+                n_fz[rr] = fz;
+            }
+            __syncthreads();
+
+            if (FCT) {
+                // ------------- A2: per-cell limiter terms at level t ---------
+                for (int r = warp; r < TY; r += NW) {  // x: cells x in [-1, TX] -> lx 1..TX+2
+                    const int ly = r + 2, lx = lane;
+                    const int i = i0 - 2 + lx;
+                    if (lx >= 1 && lx <= TX + 2 && i <= nx - 1) {
+                        float qmax, qmin, fin, fout;
+                        const float qc = AT(sQc, lx, ly);
+                        if (i == 0) {
+                            qmax = fmax_(fmax_(qc, AT(sQc, lx + 1, ly)), fmax_(AT(sQ0c, lx, ly), AT(sQ0c, lx + 1, ly)));
+                            qmin = fmin_(fmin_(qc, AT(sQc, lx + 1, ly)), fmin_(AT(sQ0c, lx, ly), AT(sQ0c, lx + 1, ly)));
+                            fin = 0.0f;
+                            fout = 0.0f;
+                        } else if (i == nx - 1) {
+                            qmax = fmax_(fmax_(AT(sQc, lx - 1, ly), qc), AT(sQ0c, lx - 1, ly));
+                            qmin = fmin_(fmin_(AT(sQc, lx - 1, ly), qc), AT(sQ0c, lx - 1, ly));
+                            fin = 0.0f;
+                            fout = 0.0f;
+                        } else {
+                            qmax = fmax_(fmax_(fmax_(AT(sQc, lx - 1, ly), qc), AT(sQc, lx + 1, ly)),
+                                         fmax_(fmax_(AT(sQ0c, lx - 1, ly), AT(sQ0c, lx, ly)), AT(sQ0c, lx + 1, ly)));
+                            qmin = fmin_(fmin_(fmin_(AT(sQc, lx - 1, ly), qc), AT(sQc, lx + 1, ly)),
+                                         fmin_(fmin_(AT(sQ0c, lx - 1, ly), AT(sQ0c, lx, ly)), AT(sQ0c, lx + 1, ly)));
+                            const float fl = AT(S_FX, lx, ly), fr = AT(S_FX, lx + 1, ly);
+                            fin = fmax_(0.0f, fl) - fmin_(0.0f, fr);
+                            fout = fmax_(0.0f, fr) - fmin_(0.0f, fl);
+                        }
+                        AT(S_BXI, lx, ly) = fct_beta(qmax - qc, fin + e15);
+                        AT(S_BXO, lx, ly) = fct_beta(qc - qmin, fout + e15);
+                    }
+                }
+                for (int r = warp; r < TY + 2; r += NW) {  // y: cells y in [-1, TY] -> ly 1..TY+2
+                    const int ly = r + 1, lx = lane;
+                    const int j = j0 - 2 + ly;
+                    if (lx >= 2 && lx < TX + 2 && j <= ny - 1) {
+                        float qmax, qmin, fin, fout;
+                        const float qc = AT(sQc, lx, ly);
+                        if (j == 0) {
+                            qmax = fmax_(fmax_(qc, AT(sQc, lx, ly + 1)), fmax_(AT(sQ0c, lx, ly), AT(sQ0c, lx, ly + 1)));
+                            qmin = fmin_(fmin_(qc, AT(sQc, lx, ly + 1)), fmin_(AT(sQ0c, lx, ly), AT(sQ0c, lx, ly + 1)));
+                            fin = 0.0f;
+                            fout = 0.0f;
+                        } else if (j == ny - 1) {
+                            qmax = fmax_(fmax_(AT(sQc, lx, ly - 1), qc), AT(sQ0c, lx, ly - 1));
+                            qmin = fmin_(fmin_(AT(sQc, lx, ly - 1), qc), AT(sQ0c, lx, ly - 1));
+                            fin = 0.0f;
+                            fout = 0.0f;
+                        } else {
+                            qmax = fmax_(fmax_(fmax_(AT(sQc, lx, ly - 1), qc), AT(sQc, lx, ly + 1)),
+                                         fmax_(fmax_(AT(sQ0c, lx, ly - 1), AT(sQ0c, lx, ly)), AT(sQ0c, lx, ly + 1)));
+                            qmin = fmin_(fmin_(fmin_(AT(sQc, lx, ly - 1), qc), AT(sQc, lx, ly + 1)),
+                                         fmin_(fmin_(AT(sQ0c, lx, ly - 1), AT(sQ0c, lx, ly)), AT(sQ0c, lx, ly + 1)));
+                            const float fl = AT(S_FY, lx, ly), fr = AT(S_FY, lx, ly + 1);
+                            fin = fmax_(0.0f, fl) - fmin_(0.0f, fr);
+                            fout = fmax_(0.0f, fr) - fmin_(0.0f, fl);
+                        }
+                        AT(S_BYI, lx, ly) = fct_beta(qmax - qc, fin + e15);
+                        AT(S_BYO, lx, ly) = fct_beta(qc - qmin, fout + e15);
+                    }
+                }
+#pragma unroll
+                for (int rr = 0; rr < RPW; rr++) {  // z: the output cell at level t
+                    const int ly = warp + NW * rr + 2, lx = lane + 2;
+                    float bzi = 0.0f, bzo = 0.0f;
+                    if (lane < TX) {
+                        float qmax, qmin, fin, fout;
+                        const float qc = AT(sQc, lx, ly), q0c = AT(sQ0c, lx, ly);
+                        if (t == 0) {
+                            const float qu = AT(sQp, lx, ly), q0u = AT(sQ0p, lx, ly);
+                            qmax = fmax_(fmax_(qc, qu), fmax_(q0c, q0u));
+                            qmin = fmin_(fmin_(qc, qu), fmin_(q0c, q0u));
+                            fin = 0.0f - fmin_(0.0f, n_fz[rr]);
+                            fout = fmax_(0.0f, n_fz[rr]);
+                        } else if (t == nz - 1) {
+                            qmax = fmax_(fmax_(r_q1dn[rr], qc), r_q0dn[rr]);
+                            qmin = fmin_(fmin_(r_q1dn[rr], qc), r_q0dn[rr]);
+                            fin = fmax_(0.0f, r_fz[rr]) - fmin_(0.0f, r_fz[rr]);
+                            fout = fin;
+                        } else {
+                            const float qu = AT(sQp, lx, ly), q0u = AT(sQ0p, lx, ly);
+                            qmax = fmax_(fmax_(fmax_(r_q1dn[rr], qc), qu), fmax_(fmax_(r_q0dn[rr], q0c), q0u));
+                            qmin = fmin_(fmin_(fmin_(r_q1dn[rr], qc), qu), fmin_(fmin_(r_q0dn[rr], q0c), q0u));
+                            fin = fmax_(0.0f, r_fz[rr]) - fmin_(0.0f, n_fz[rr]);
+                            fout = fmax_(0.0f, n_fz[rr]) - fmin_(0.0f, r_fz[rr]);
+                        }
+                        bzi = fct_beta(qmax - qc, fin + e15);
+                        bzo = fct_beta(qc - qmin, fout + e15);
+                    }
+                    n_bzi[rr] = bzi;
+                    n_bzo[rr] = bzo;
+                }
+                __syncthreads();
+            }
+            // ---------------- A3: limited u2, v2 at level t -------------------
+            float *u2l = P(S_U2L + (t & 1)), *v2l = P(S_V2L + (t & 1));
+            for (int r = warp; r < TY; r += NW) {  // faces x in [0, TX] -> lx 2..TX+2
+                const int ly = r + 2, lx = lane;
+                if (lx >= 2 && lx <= TX + 2) {
+                    float u = AT(S_U2, lx, ly);
+                    if (FCT) {
+                        if (u > 0.0f)
+                            u = fmin_(fmin_(1.0f, AT(S_BXI, lx, ly)), AT(S_BXO, lx - 1, ly)) * u;
+                        else if (u < 0.0f)
+                            u = fmin_(fmin_(1.0f, AT(S_BXI, lx - 1, ly)), AT(S_BXO, lx, ly)) * u;
+                    }
+                    u2l[ly * PW + lx] = u;
+                }
+            }
+            for (int r = warp; r < TY + 1; r += NW) {  // faces y in [0, TY] -> ly 2..TY+2
+                const int ly = r + 2, lx = lane;
+                if (lx >= 2 && lx < TX + 2) {
+                    float v = AT(S_V2, lx, ly);
+                    if (FCT) {
+                        if (v > 0.0f)
+                            v = fmin_(fmin_(1.0f, AT(S_BYI, lx, ly)), AT(S_BYO, lx, ly - 1)) * v;
+                        else if (v < 0.0f)
+                            v = fmin_(fmin_(1.0f, AT(S_BYI, lx, ly - 1)), AT(S_BYO, lx, ly)) * v;
+                    }
+                    v2l[ly * PW + lx] = v;
+                }
+            }
+            // limited w2 at the top face of level t-1
+#pragma unroll
+            for (int rr = 0; rr < RPW; rr++) {
+                float w = r_w2[rr];
+                if (FCT && t >= 1) {
+                    if (w > 0.0f)
+                        w = fmin_(fmin_(1.0f, n_bzi[rr]), r_bzo[rr]) * w;
+                    else if (w < 0.0f)
+                        w = fmin_(fmin_(1.0f, r_bzi[rr]), n_bzo[rr]) * w;
+                }
+                n_w2l[rr] = w;
+            }
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < RPW; rr++) {
+                n_w2l[rr] = 0.0f;  // top face of the model: w2(kme) = 0
+                n_fz[rr] = n_w2[rr] = n_bzi[rr] = n_bzo[rr] = 0.0f;
+            }
+        }
+
+        // ---------------- B: corrective donor-cell pass at level t-1 ----------
+        if (t >= 1) {
+            const int L = t - 1;
+            const int sQL = sQm;  // q1 plane of level t-1
+            const float *u2l = P(S_U2L + (L & 1)), *v2l = P(S_V2L + (L & 1));
+#pragma unroll
+            for (int rr = 0; rr < RPW; rr++) {
+                const int ly = warp + NW * rr + 2, lx = lane + 2;
+                const int i = i0 - 2 + lx, j = j0 - 2 + ly;
+                if (lane < TX && i <= nx - 2 && j <= ny - 2) {
+                    const float qc = AT(sQL, lx, ly);
+                    const float fe = flux1(qc, AT(sQL, lx + 1, ly), u2l[ly * PW + lx + 1]);
+                    const float fw = flux1(AT(sQL, lx - 1, ly), qc, u2l[ly * PW + lx]);
+                    const float f3 = flux1(qc, AT(sQL, lx, ly + 1), v2l[(ly + 1) * PW + lx]);
+                    const float f4 = flux1(AT(sQL, lx, ly - 1), qc, v2l[ly * PW + lx]);
+                    float val = qc - ((fe - fw) + (f3 - f4)) / r_G[rr];
+                    const float wtop = n_w2l[rr], wbot = r_w2l[rr];
+                    if (L > 0 && L < nz - 1) {
+                        const float f5t = flux1(qc, AT(sQc, lx, ly), wtop);
+                        const float f5b = flux1(r_q1dd[rr], qc, wbot);
+                        val = val - (f5t - f5b) / r_DJR[rr];
+                    } else if (L == 0) {
+                        const float f5t = flux1(qc, AT(sQc, lx, ly), wtop);
+                        val = val - f5t / r_DJR[rr];
+                    } else {
+                        const float f5b = flux1(r_q1dd[rr], qc, wbot);
+                        val = val - (qc * wtop - f5b) / r_DJR[rr];
+                    }
+                    outg[ix(g, i, L, j)] = val;
+                }
+            }
+        }
+
+        // ---------------- rotate the per-cell z state ------------------------
+        if (haveA) {
+#pragma unroll
+            for (int rr = 0; rr < RPW; rr++) {
+                const int ly = warp + NW * rr + 2, lx = lane + 2;
+                const int i = min(i0 - 2 + lx, nx - 1), j = min(j0 - 2 + ly, ny - 1);
+                r_q1dd[rr] = r_q1dn[rr];
+                r_q1dn[rr] = AT(sQc, lx, ly);   // q1 at level t, "below" for level t+1
+                r_q0dn[rr] = AT(sQ0c, lx, ly);
+                r_fz[rr] = n_fz[rr];
+                r_w2[rr] = n_w2[rr];
+                r_bzi[rr] = n_bzi[rr];
+                r_bzo[rr] = n_bzo[rr];
+                r_w2l[rr] = n_w2l[rr];
+                r_G[rr] = AT(sGc, lx, ly);
+                r_DJR[rr] = DJR[ix(g, i, t, j)];
+            }
+        }
+    }
+#undef AT
+}
+
+inline bool fused_eligible(int order, int fct) { return order == 2 && (fct == 0 || fct == 1); }
+
+inline int mp_tiles_x(const Geo &g) { return (g.nx - 2 + mpf::TX - 1) / mpf::TX; }
+inline int mp_tiles_y(const Geo &g) { return (g.ny - 2 + mpf::TY - 1) / mpf::TY; }
 
 // Debug check (parameters%debug): flags any interior cell whose donor-cell
 // outflow fraction, sum of outgoing Courant fluxes over J*rho (dz*J*rho for

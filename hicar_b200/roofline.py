@@ -5,8 +5,8 @@ read and written once (8 B per cell-species) and the eight species-
 independent fields (u, v, w, density, jacobian, jacobian_u/_v/_w) are read
 once per step (32 B per cell), shared by the S species:
     8 + 32/S bytes per cell-species  (10.67 B at S=12, 40 B at S=1).
-One species pass therefore moves cells * (8 + 32/S) algorithmic bytes.
-advection_dz is one value per level and is not counted.
+One advect call (all S species) therefore moves cells * (8*S + 32)
+algorithmic bytes.  advection_dz is one value per level and is not counted.
 """
 from __future__ import annotations
 
@@ -30,9 +30,10 @@ def bytes_per_cell_species(S: int) -> float:
 
 
 def species_pass(nx: int, ny: int, nz: int, S: int, total_ms: float, passes: int, traffic=None) -> dict:
-    """Roofline entry for the per-species advection pass (the dominant kernel)."""
+    """Roofline entry for the advection kernels of one advect call (all S
+    species), timed with CUDA events on the launching stream."""
     peak, kind = hbm_peak()
-    per_pass = nx * ny * nz * bytes_per_cell_species(S)
+    per_pass = nx * ny * nz * S * bytes_per_cell_species(S)
     if passes <= 0 or total_ms <= 0:
         achieved = None
     else:
@@ -42,5 +43,5 @@ def species_pass(nx: int, ny: int, nz: int, S: int, total_ms: float, passes: int
         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
         "peak_kind": kind, "algorithmic_bytes_per_launch": per_pass,
         "launch_ms": (total_ms / passes) if passes else None,
-        "bytes_model": "8 + 32/S B per cell-species, one species pass per launch",
+        "bytes_model": "8 + 32/S B per cell-species; one launch = the kernels of one advect call",
     }

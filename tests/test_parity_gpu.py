@@ -182,3 +182,24 @@ def test_closed_domain_mass_gpu(oracle_lib):
     m = lambda q: float((q.astype(np.float64) * case.jacobian * case.density * case.advection_dz).sum())
     out = gpu_run(case, Options(), 50)
     assert abs(m(out["qv"]) - m(case.species["qv"])) / m(case.species["qv"]) < 2e-6
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(3, 3, 3), (30, 18, 3), (29, 17, 5), (57, 33, 7), (100, 70, 41), (31, 200, 4)])
+def test_fused_matches_oracle_on_ragged_shapes(oracle_lib, nx, ny, nz):
+    """Tile edges of the fused kernel (28x16 column tiles) at every offset,
+    the smallest legal domain and short/tall columns."""
+    O = oracle_lib
+    case = synth.config2(seed=nx + ny + nz, nx=nx, ny=ny, nz=nz)
+    case.species = {k: case.species[k] for k in ("qv", "qc", "nr", "theta")}
+    for fct in (1, 0):
+        o = O.make_opts(mpdata_fct=fct)
+        ref = O.run_steps(case, o, case.dt, 3)
+        assert_exact(gpu_run(case, options_from(o), 3), ref, label=f"{nx}x{ny}x{nz} fct={fct} ")
+
+
+def test_fused_and_staged_agree_over_many_steps(oracle_lib):
+    case = synth.config2(seed=21, nx=90, ny=75, nz=20)
+    a = gpu_run(case, Options(), 40)
+    b = gpu_run(case, Options(), 40, staged=True)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
