@@ -43,7 +43,7 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="full_species", choices=["full_species", "plain_c1"])
+    p.add_argument("--workload", default="full_species", choices=["full_species", "plain_c1", "mid_species"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
     p.add_argument("--quick", action="store_true",
@@ -55,6 +55,9 @@ def make_case(workload: str, seed: int):
     from hicar_b200 import synth
     if workload == "plain_c1":
         return synth.config1(seed=seed), "plain MPDATA single domain 128x128x20, 1 field (qv), dt 20 s"
+    if workload == "mid_species":
+        return (synth.config2(seed=seed, nx=256, ny=256, nz=40),
+                "full-species domain at quarter area 256x256x40, 12 fields, dt 4 s (profiling case)")
     return synth.config2(seed=seed), "full-species single domain 512x512x40, 12 fields, dt 4 s"
 
 
