@@ -208,7 +208,10 @@ def run_b200(args):
     adv_init(d, opts)
     if args.staged:
         d.use_staged_kernels(True)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library and the timing events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
     L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
     h = d.handle
 

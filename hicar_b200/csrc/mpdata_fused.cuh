@@ -146,19 +146,19 @@ constexpr int S_U = 7;            // U_m, 3 slots
 constexpr int S_V = 10;           // V_m, 3 slots
 constexpr int S_W = 13;           // W' = W_m/dz, 3 slots
 constexpr int S_G = 16;           // G = J*rho, 3 slots
-constexpr int S_U2 = 19, S_FX = 20, S_V2 = 21, S_FY = 22;
-constexpr int S_BXI = 23, S_BXO = 24, S_BYI = 25, S_BYO = 26;
-constexpr int S_U2L = 27;         // 2 ring slots
-constexpr int S_V2L = 29;         // 2 ring slots
-constexpr int NPLANES = 31;
+constexpr int S_U2 = 19, S_V2 = 20;  // unlimited pseudo-velocities of level t
+constexpr int S_BXI = 21, S_BXO = 22, S_BYI = 23, S_BYO = 24;
+constexpr int S_U2L = 25;         // 2 ring slots
+constexpr int S_V2L = 27;         // 2 ring slots
+constexpr int NPLANES = 29;
 constexpr size_t SMEM = (size_t)NPLANES * PLANE * sizeof(float);
 }  // namespace mpf
 
-__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid)
+__device__ __forceinline__ void cp_async16(float *dst, const float *src, bool valid)
 {
     unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    int n = valid ? 4 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n));
+    int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -175,22 +175,33 @@ __device__ __forceinline__ float fct_beta(float num, float den)
     return num / den;
 }
 
-// Asynchronously copy level `lev` of a 3-D field into a plane slot.  ex/ey
-// are the valid x/y extents of the field (nx or nx+1, ny or ny+1); cells
-// outside read as zero.
+// Asynchronously copy level `lev` of a 3-D field into a plane slot, in
+// 16-byte chunks: the plane starts at x = i0-2, a multiple of 4, so every
+// chunk is either wholly inside a row's pitch (valid cells, or the zero
+// padding past nx) or wholly outside the field and zero-filled.  ey is the
+// y extent of the field (ny, or ny+1 for y-face fields).
 __device__ __forceinline__ void load_plane(float *dst, const float *__restrict__ src, const Geo &g, int lev, int i0,
-                                           int j0, int ex, int ey)
+                                           int j0, int ey)
 {
-    for (int e = threadIdx.x; e < mpf::PLANE; e += mpf::NT) {
-        const int lx = e % mpf::PW, ly = e / mpf::PW;
-        const int i = i0 - 2 + lx, j = j0 - 2 + ly;
-        const bool ok = i >= 0 && i < ex && j >= 0 && j < ey;
-        cp_async4(dst + e, ok ? src + ix(g, i, lev, j) : src, ok);
+    for (int e = threadIdx.x; e < (mpf::PW / 4) * mpf::PH; e += mpf::NT) {
+        const int cx = e % (mpf::PW / 4), ly = e / (mpf::PW / 4);
+        const int i = i0 - 2 + 4 * cx, j = j0 - 2 + ly;
+        const bool ok = i >= 0 && i < g.P && j >= 0 && j < ey;
+        cp_async16(dst + ly * mpf::PW + 4 * cx, ok ? src + ix(g, i, lev, j) : src, ok);
     }
 }
 
+// q/d for the limiter-free divisions of the pseudo-velocity and corrective
+// passes; a zero numerator over a positive denominator is returned as is
+// (the exact IEEE quotient), which skips the division in empty regions.
+__device__ __forceinline__ float div0(float n, float d)
+{
+    if (n == 0.0f && d > 0.0f) return n;
+    return n / d;
+}
+
 template <bool FCT>
-__global__ void __launch_bounds__(mpf::NT, 2)
+__global__ void __launch_bounds__(mpf::NT, 3)
     k_mp_corr(Geo g, SpeciesPtrs sp, int nspecies, int tiles_x, const float *__restrict__ Um,
               const float *__restrict__ Vm, const float *__restrict__ Wp, const float *__restrict__ Gc,
               const float *__restrict__ DJR, const float *__restrict__ dz)
@@ -199,7 +210,7 @@ __global__ void __launch_bounds__(mpf::NT, 2)
     extern __shared__ float sm[];
     const int s = blockIdx.x % nspecies;
     const int tile = blockIdx.x / nspecies;
-    const int i0 = 1 + (tile % tiles_x) * TX;  // first output column (interior starts at 1)
+    const int i0 = (tile % tiles_x) * TX - 2;  // first output column; i0-2 is a multiple of 4
     const int j0 = 1 + (tile / tiles_x) * TY;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const float *__restrict__ q0g = sp.q0[s];
@@ -211,17 +222,17 @@ __global__ void __launch_bounds__(mpf::NT, 2)
 #define AT(slot, lx, ly) sm[(size_t)(slot) * PLANE + (ly) * PW + (lx)]
 
     // ---- prologue: levels 0 and 1 of everything the first iteration reads
-    load_plane(P(S_Q1 + 0), q1g, g, 0, i0, j0, nx, ny);
-    load_plane(P(S_Q0 + 0), q0g, g, 0, i0, j0, nx, ny);
-    load_plane(P(S_U + 0), Um, g, 0, i0, j0, nx + 1, ny);
-    load_plane(P(S_V + 0), Vm, g, 0, i0, j0, nx, ny + 1);
-    load_plane(P(S_W + 0), Wp, g, 0, i0, j0, nx, ny);
-    load_plane(P(S_G + 0), Gc, g, 0, i0, j0, nx, ny);
-    load_plane(P(S_Q1 + 1), q1g, g, 1, i0, j0, nx, ny);
-    load_plane(P(S_Q0 + 1), q0g, g, 1, i0, j0, nx, ny);
-    load_plane(P(S_U + 1), Um, g, 1, i0, j0, nx + 1, ny);
-    load_plane(P(S_V + 1), Vm, g, 1, i0, j0, nx, ny + 1);
-    load_plane(P(S_G + 1), Gc, g, 1, i0, j0, nx, ny);
+    load_plane(P(S_Q1 + 0), q1g, g, 0, i0, j0, ny);
+    load_plane(P(S_Q0 + 0), q0g, g, 0, i0, j0, ny);
+    load_plane(P(S_U + 0), Um, g, 0, i0, j0, ny);
+    load_plane(P(S_V + 0), Vm, g, 0, i0, j0, ny + 1);
+    load_plane(P(S_W + 0), Wp, g, 0, i0, j0, ny);
+    load_plane(P(S_G + 0), Gc, g, 0, i0, j0, ny);
+    load_plane(P(S_Q1 + 1), q1g, g, 1, i0, j0, ny);
+    load_plane(P(S_Q0 + 1), q0g, g, 1, i0, j0, ny);
+    load_plane(P(S_U + 1), Um, g, 1, i0, j0, ny);
+    load_plane(P(S_V + 1), Vm, g, 1, i0, j0, ny + 1);
+    load_plane(P(S_G + 1), Gc, g, 1, i0, j0, ny);
     cp_async_commit();
 
     // per-output-cell z state (two output rows per warp)
@@ -241,13 +252,13 @@ __global__ void __launch_bounds__(mpf::NT, 2)
         __syncthreads();
         // prefetch the levels the next iteration adds: q1/q0/U/V/G at t+2, W' at t+1
         if (t + 2 < nz) {
-            load_plane(P(S_Q1 + ((t + 2) & 3)), q1g, g, t + 2, i0, j0, nx, ny);
-            load_plane(P(S_Q0 + (t + 2) % 3), q0g, g, t + 2, i0, j0, nx, ny);
-            load_plane(P(S_U + (t + 2) % 3), Um, g, t + 2, i0, j0, nx + 1, ny);
-            load_plane(P(S_V + (t + 2) % 3), Vm, g, t + 2, i0, j0, nx, ny + 1);
-            load_plane(P(S_G + (t + 2) % 3), Gc, g, t + 2, i0, j0, nx, ny);
+            load_plane(P(S_Q1 + ((t + 2) & 3)), q1g, g, t + 2, i0, j0, ny);
+            load_plane(P(S_Q0 + (t + 2) % 3), q0g, g, t + 2, i0, j0, ny);
+            load_plane(P(S_U + (t + 2) % 3), Um, g, t + 2, i0, j0, ny);
+            load_plane(P(S_V + (t + 2) % 3), Vm, g, t + 2, i0, j0, ny + 1);
+            load_plane(P(S_G + (t + 2) % 3), Gc, g, t + 2, i0, j0, ny);
         }
-        if (t + 1 < nz) load_plane(P(S_W + (t + 1) % 3), Wp, g, t + 1, i0, j0, nx, ny);
+        if (t + 1 < nz) load_plane(P(S_W + (t + 1) % 3), Wp, g, t + 1, i0, j0, ny);
         cp_async_commit();
 
         const bool haveA = t < nz;
@@ -265,99 +276,95 @@ __global__ void __launch_bounds__(mpf::NT, 2)
             for (int r = warp; r < TY; r += NW) {  // u2 faces x in [-1, TX+1] -> lx 1..31
                 const int ly = r + 2, lx = lane;
                 const int f = i0 - 2 + lx, j = j0 - 2 + ly;
-                float u2 = 0.0f, fx = 0.0f;
+                float u2 = 0.0f;
                 if (lx >= 1 && f >= 1 && f <= nx - 1 && j <= ny - 1) {
                     const float rx = AT(sQc, lx, ly), lq = AT(sQc, lx - 1, ly);
                     const float uu = AT(sUc, lx, ly);
                     const float Gs = AT(sGc, lx, ly) + AT(sGc, lx - 1, ly);
                     const float denom = rx + lq + e10;
                     float val = fabsf(uu) * (1.0f - fabsf(uu) / (0.5f * Gs));
-                    val = val * (rx - lq) / denom;
+                    val = div0(val * (rx - lq), denom);
                     if (j > 0 && j < ny - 1) {
                         const float a = AT(sQc, lx, ly + 1), b = AT(sQc, lx, ly - 1);
                         const float c = AT(sQc, lx - 1, ly + 1), d = AT(sQc, lx - 1, ly - 1);
-                        const float eq = (a - b + c - d) / (a + b + c + d + e10);
+                        const float eq = div0(a - b + c - d, a + b + c + d + e10);
                         const float ev = q4 * (AT(sVc, lx, ly) + AT(sVc, lx, ly + 1) + AT(sVc, lx - 1, ly) +
                                                AT(sVc, lx - 1, ly + 1));
-                        val = val - 0.5f * uu * ev * eq / Gs;
+                        val = val - div0(0.5f * uu * ev * eq, Gs);
                     }
                     if (kint) {
                         const float a = AT(sQp, lx, ly), b = AT(sQm, lx, ly);
                         const float c = AT(sQp, lx - 1, ly), d = AT(sQm, lx - 1, ly);
-                        const float eq = (a - b + c - d) / (a + b + c + d + e10);
+                        const float eq = div0(a - b + c - d, a + b + c + d + e10);
                         const float ev = q4 * (AT(sWc, lx, ly) + AT(sWm, lx, ly) + AT(sWc, lx - 1, ly) +
                                                AT(sWm, lx - 1, ly));
-                        val = val - 0.5f * uu * ev * eq / Gs;
+                        val = val - div0(0.5f * uu * ev * eq, Gs);
                     }
                     u2 = val * 0.5f;
-                    fx = flux1(lq, rx, u2);
                 }
                 AT(S_U2, lx, ly) = u2;
-                AT(S_FX, lx, ly) = fx;
             }
             for (int r = warp; r < TY + 3; r += NW) {  // v2 faces y in [-1, TY+1] -> ly 1..TY+3
                 const int ly = r + 1, lx = lane;
                 const int i = i0 - 2 + lx, gf = j0 - 2 + ly;
-                float v2 = 0.0f, fy = 0.0f;
-                if (lx >= 2 && lx < TX + 2 && i <= nx - 1 && gf >= 1 && gf <= ny - 1) {
+                float v2 = 0.0f;
+                if (lx >= 2 && lx < TX + 2 && i >= 0 && i <= nx - 1 && gf >= 1 && gf <= ny - 1) {
                     const float rq = AT(sQc, lx, ly), lq = AT(sQc, lx, ly - 1);
                     const float vv = AT(sVc, lx, ly);
                     const float Gs = AT(sGc, lx, ly) + AT(sGc, lx, ly - 1);
                     const float denom = rq + lq + e10;
                     float val = fabsf(vv) * (1.0f - fabsf(vv) / (0.5f * Gs));
-                    val = val * (rq - lq) / denom;
+                    val = div0(val * (rq - lq), denom);
                     float ev = 0.0f, eq = 0.0f;
                     if (i > 0 && i < nx - 1) {
                         const float A = AT(sQc, lx + 1, ly - 1), B = AT(sQc, lx - 1, ly);
                         const float C = AT(sQc, lx + 1, ly), D = AT(sQc, lx - 1, ly - 1);
-                        eq = (A - B + C - D) / (C + A + B + D + e10);
+                        eq = div0(A - B + C - D, C + A + B + D + e10);
                         ev = q4 * (AT(sUc, lx + 1, ly) + AT(sUc, lx + 1, ly - 1) + AT(sUc, lx, ly) +
                                    AT(sUc, lx, ly - 1));
                     }
-                    val = val - 0.5f * vv * ev * eq / Gs;
+                    val = val - div0(0.5f * vv * ev * eq, Gs);
                     if (kint) {
                         const float A = AT(sQp, lx, ly - 1), B = AT(sQm, lx, ly);
                         const float C = AT(sQp, lx, ly), D = AT(sQm, lx, ly - 1);
-                        const float eq2 = (A - B + C - D) / (A + B + C + D + e10);
+                        const float eq2 = div0(A - B + C - D, A + B + C + D + e10);
                         const float ev2 = q4 * (AT(sWc, lx, ly) + AT(sWm, lx, ly) + AT(sWc, lx, ly - 1) +
                                                 AT(sWm, lx, ly - 1));
-                        val = val - 0.5f * vv * ev2 * eq2 / Gs;
+                        val = val - div0(0.5f * vv * ev2 * eq2, Gs);
                     }
                     v2 = val * 0.5f;
-                    fy = flux1(lq, rq, v2);
                 }
                 AT(S_V2, lx, ly) = v2;
-                AT(S_FY, lx, ly) = fy;
             }
 #pragma unroll
             for (int rr = 0; rr < RPW; rr++) {  // w2 at the top face of level t, output cells
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
                 float w2 = 0.0f, fz = 0.0f;
-                if (lane < TX && t < nz - 1) {
+                const int iw = i0 - 2 + lx, jw = j0 - 2 + ly;
+                if (lane < TX && t < nz - 1 && iw >= 1 && iw <= nx - 2 && jw <= ny - 2) {
                     const float rq = AT(sQp, lx, ly), lq = AT(sQc, lx, ly);
                     const float ww = AT(sWc, lx, ly);
                     const float Gs = AT(sGp, lx, ly) + AT(sGc, lx, ly);
                     const float denom = rq + lq + e10;
                     float val = fabsf(ww) * (1.0f - fabsf(ww) / (0.5f * Gs));
-                    val = val * (rq - lq) / denom;
+                    val = div0(val * (rq - lq), denom);
                     {
                         const float A = AT(sQp, lx + 1, ly), B = AT(sQc, lx - 1, ly);
                         const float C = AT(sQc, lx + 1, ly), D = AT(sQp, lx - 1, ly);
-                        const float eq = (A - B + C - D) / (C + A + B + D + e10);
+                        const float eq = div0(A - B + C - D, C + A + B + D + e10);
                         const float ev = q4 * (AT(sUc, lx + 1, ly) + AT(sUp, lx + 1, ly) + AT(sUc, lx, ly) +
                                                AT(sUp, lx, ly));
-                        val = val - 0.5f * ww * ev * eq / Gs;
+                        val = val - div0(0.5f * ww * ev * eq, Gs);
                     }
                     {
                         const float A = AT(sQp, lx, ly + 1), B = AT(sQc, lx, ly - 1);
                         const float C = AT(sQc, lx, ly + 1), D = AT(sQp, lx, ly - 1);
-                        const float eq2 = (A - B + C - D) / (C + D + A + B + e10);
+                        const float eq2 = div0(A - B + C - D, C + D + A + B + e10);
                         const float ev2 = q4 * (AT(sVc, lx, ly) + AT(sVp, lx, ly) + AT(sVc, lx, ly + 1) +
                                                 AT(sVp, lx, ly + 1));
-                        val = val - 0.5f * ww * ev2 * eq2 / Gs;
+                        val = val - div0(0.5f * ww * ev2 * eq2, Gs);
                     }
-                    const int i = i0 - 2 + lx, j = j0 - 2 + ly;
-                    w2 = val * 0.5f * dz[ix(g, min(i, nx - 1), t, min(j, ny - 1))];
+                    w2 = val * 0.5f * dz[ix(g, iw, t, jw)];
                     fz = flux1(lq, rq, w2);
                 }
                 n_w2[rr] = w2;
@@ -370,27 +377,28 @@ __global__ void __launch_bounds__(mpf::NT, 2)
                 for (int r = warp; r < TY; r += NW) {  // x: cells x in [-1, TX] -> lx 1..TX+2
                     const int ly = r + 2, lx = lane;
                     const int i = i0 - 2 + lx;
-                    if (lx >= 1 && lx <= TX + 2 && i <= nx - 1) {
+                    if (lx >= 1 && lx <= TX + 2 && i >= 0 && i <= nx - 1) {
                         float qmax, qmin, fin, fout;
                         const float qc = AT(sQc, lx, ly);
                         if (i == 0) {
-                            qmax = fmax_(fmax_(qc, AT(sQc, lx + 1, ly)), fmax_(AT(sQ0c, lx, ly), AT(sQ0c, lx + 1, ly)));
-                            qmin = fmin_(fmin_(qc, AT(sQc, lx + 1, ly)), fmin_(AT(sQ0c, lx, ly), AT(sQ0c, lx + 1, ly)));
+                            qmax = fmaxf(fmaxf(qc, AT(sQc, lx + 1, ly)), fmaxf(AT(sQ0c, lx, ly), AT(sQ0c, lx + 1, ly)));
+                            qmin = fminf(fminf(qc, AT(sQc, lx + 1, ly)), fminf(AT(sQ0c, lx, ly), AT(sQ0c, lx + 1, ly)));
                             fin = 0.0f;
                             fout = 0.0f;
                         } else if (i == nx - 1) {
-                            qmax = fmax_(fmax_(AT(sQc, lx - 1, ly), qc), AT(sQ0c, lx - 1, ly));
-                            qmin = fmin_(fmin_(AT(sQc, lx - 1, ly), qc), AT(sQ0c, lx - 1, ly));
+                            qmax = fmaxf(fmaxf(AT(sQc, lx - 1, ly), qc), AT(sQ0c, lx - 1, ly));
+                            qmin = fminf(fminf(AT(sQc, lx - 1, ly), qc), AT(sQ0c, lx - 1, ly));
                             fin = 0.0f;
                             fout = 0.0f;
                         } else {
-                            qmax = fmax_(fmax_(fmax_(AT(sQc, lx - 1, ly), qc), AT(sQc, lx + 1, ly)),
-                                         fmax_(fmax_(AT(sQ0c, lx - 1, ly), AT(sQ0c, lx, ly)), AT(sQ0c, lx + 1, ly)));
-                            qmin = fmin_(fmin_(fmin_(AT(sQc, lx - 1, ly), qc), AT(sQc, lx + 1, ly)),
-                                         fmin_(fmin_(AT(sQ0c, lx - 1, ly), AT(sQ0c, lx, ly)), AT(sQ0c, lx + 1, ly)));
-                            const float fl = AT(S_FX, lx, ly), fr = AT(S_FX, lx + 1, ly);
-                            fin = fmax_(0.0f, fl) - fmin_(0.0f, fr);
-                            fout = fmax_(0.0f, fr) - fmin_(0.0f, fl);
+                            qmax = fmaxf(fmaxf(fmaxf(AT(sQc, lx - 1, ly), qc), AT(sQc, lx + 1, ly)),
+                                         fmaxf(fmaxf(AT(sQ0c, lx - 1, ly), AT(sQ0c, lx, ly)), AT(sQ0c, lx + 1, ly)));
+                            qmin = fminf(fminf(fminf(AT(sQc, lx - 1, ly), qc), AT(sQc, lx + 1, ly)),
+                                         fminf(fminf(AT(sQ0c, lx - 1, ly), AT(sQ0c, lx, ly)), AT(sQ0c, lx + 1, ly)));
+                            const float fl = flux1(AT(sQc, lx - 1, ly), qc, AT(S_U2, lx, ly));
+                            const float fr = flux1(qc, AT(sQc, lx + 1, ly), AT(S_U2, lx + 1, ly));
+                            fin = fmaxf(0.0f, fl) - fminf(0.0f, fr);
+                            fout = fmaxf(0.0f, fr) - fminf(0.0f, fl);
                         }
                         AT(S_BXI, lx, ly) = fct_beta(qmax - qc, fin + e15);
                         AT(S_BXO, lx, ly) = fct_beta(qc - qmin, fout + e15);
@@ -403,23 +411,24 @@ __global__ void __launch_bounds__(mpf::NT, 2)
                         float qmax, qmin, fin, fout;
                         const float qc = AT(sQc, lx, ly);
                         if (j == 0) {
-                            qmax = fmax_(fmax_(qc, AT(sQc, lx, ly + 1)), fmax_(AT(sQ0c, lx, ly), AT(sQ0c, lx, ly + 1)));
-                            qmin = fmin_(fmin_(qc, AT(sQc, lx, ly + 1)), fmin_(AT(sQ0c, lx, ly), AT(sQ0c, lx, ly + 1)));
+                            qmax = fmaxf(fmaxf(qc, AT(sQc, lx, ly + 1)), fmaxf(AT(sQ0c, lx, ly), AT(sQ0c, lx, ly + 1)));
+                            qmin = fminf(fminf(qc, AT(sQc, lx, ly + 1)), fminf(AT(sQ0c, lx, ly), AT(sQ0c, lx, ly + 1)));
                             fin = 0.0f;
                             fout = 0.0f;
                         } else if (j == ny - 1) {
-                            qmax = fmax_(fmax_(AT(sQc, lx, ly - 1), qc), AT(sQ0c, lx, ly - 1));
-                            qmin = fmin_(fmin_(AT(sQc, lx, ly - 1), qc), AT(sQ0c, lx, ly - 1));
+                            qmax = fmaxf(fmaxf(AT(sQc, lx, ly - 1), qc), AT(sQ0c, lx, ly - 1));
+                            qmin = fminf(fminf(AT(sQc, lx, ly - 1), qc), AT(sQ0c, lx, ly - 1));
                             fin = 0.0f;
                             fout = 0.0f;
                         } else {
-                            qmax = fmax_(fmax_(fmax_(AT(sQc, lx, ly - 1), qc), AT(sQc, lx, ly + 1)),
-                                         fmax_(fmax_(AT(sQ0c, lx, ly - 1), AT(sQ0c, lx, ly)), AT(sQ0c, lx, ly + 1)));
-                            qmin = fmin_(fmin_(fmin_(AT(sQc, lx, ly - 1), qc), AT(sQc, lx, ly + 1)),
-                                         fmin_(fmin_(AT(sQ0c, lx, ly - 1), AT(sQ0c, lx, ly)), AT(sQ0c, lx, ly + 1)));
-                            const float fl = AT(S_FY, lx, ly), fr = AT(S_FY, lx, ly + 1);
-                            fin = fmax_(0.0f, fl) - fmin_(0.0f, fr);
-                            fout = fmax_(0.0f, fr) - fmin_(0.0f, fl);
+                            qmax = fmaxf(fmaxf(fmaxf(AT(sQc, lx, ly - 1), qc), AT(sQc, lx, ly + 1)),
+                                         fmaxf(fmaxf(AT(sQ0c, lx, ly - 1), AT(sQ0c, lx, ly)), AT(sQ0c, lx, ly + 1)));
+                            qmin = fminf(fminf(fminf(AT(sQc, lx, ly - 1), qc), AT(sQc, lx, ly + 1)),
+                                         fminf(fminf(AT(sQ0c, lx, ly - 1), AT(sQ0c, lx, ly)), AT(sQ0c, lx, ly + 1)));
+                            const float fl = flux1(AT(sQc, lx, ly - 1), qc, AT(S_V2, lx, ly));
+                            const float fr = flux1(qc, AT(sQc, lx, ly + 1), AT(S_V2, lx, ly + 1));
+                            fin = fmaxf(0.0f, fl) - fminf(0.0f, fr);
+                            fout = fmaxf(0.0f, fr) - fminf(0.0f, fl);
                         }
                         AT(S_BYI, lx, ly) = fct_beta(qmax - qc, fin + e15);
                         AT(S_BYO, lx, ly) = fct_beta(qc - qmin, fout + e15);
@@ -434,21 +443,21 @@ __global__ void __launch_bounds__(mpf::NT, 2)
                         const float qc = AT(sQc, lx, ly), q0c = AT(sQ0c, lx, ly);
                         if (t == 0) {
                             const float qu = AT(sQp, lx, ly), q0u = AT(sQ0p, lx, ly);
-                            qmax = fmax_(fmax_(qc, qu), fmax_(q0c, q0u));
-                            qmin = fmin_(fmin_(qc, qu), fmin_(q0c, q0u));
-                            fin = 0.0f - fmin_(0.0f, n_fz[rr]);
-                            fout = fmax_(0.0f, n_fz[rr]);
+                            qmax = fmaxf(fmaxf(qc, qu), fmaxf(q0c, q0u));
+                            qmin = fminf(fminf(qc, qu), fminf(q0c, q0u));
+                            fin = 0.0f - fminf(0.0f, n_fz[rr]);
+                            fout = fmaxf(0.0f, n_fz[rr]);
                         } else if (t == nz - 1) {
-                            qmax = fmax_(fmax_(r_q1dn[rr], qc), r_q0dn[rr]);
-                            qmin = fmin_(fmin_(r_q1dn[rr], qc), r_q0dn[rr]);
-                            fin = fmax_(0.0f, r_fz[rr]) - fmin_(0.0f, r_fz[rr]);
+                            qmax = fmaxf(fmaxf(r_q1dn[rr], qc), r_q0dn[rr]);
+                            qmin = fminf(fminf(r_q1dn[rr], qc), r_q0dn[rr]);
+                            fin = fmaxf(0.0f, r_fz[rr]) - fminf(0.0f, r_fz[rr]);
                             fout = fin;
                         } else {
                             const float qu = AT(sQp, lx, ly), q0u = AT(sQ0p, lx, ly);
-                            qmax = fmax_(fmax_(fmax_(r_q1dn[rr], qc), qu), fmax_(fmax_(r_q0dn[rr], q0c), q0u));
-                            qmin = fmin_(fmin_(fmin_(r_q1dn[rr], qc), qu), fmin_(fmin_(r_q0dn[rr], q0c), q0u));
-                            fin = fmax_(0.0f, r_fz[rr]) - fmin_(0.0f, n_fz[rr]);
-                            fout = fmax_(0.0f, n_fz[rr]) - fmin_(0.0f, r_fz[rr]);
+                            qmax = fmaxf(fmaxf(fmaxf(r_q1dn[rr], qc), qu), fmaxf(fmaxf(r_q0dn[rr], q0c), q0u));
+                            qmin = fminf(fminf(fminf(r_q1dn[rr], qc), qu), fminf(fminf(r_q0dn[rr], q0c), q0u));
+                            fin = fmaxf(0.0f, r_fz[rr]) - fminf(0.0f, n_fz[rr]);
+                            fout = fmaxf(0.0f, n_fz[rr]) - fminf(0.0f, r_fz[rr]);
                         }
                         bzi = fct_beta(qmax - qc, fin + e15);
                         bzo = fct_beta(qc - qmin, fout + e15);
@@ -466,9 +475,9 @@ __global__ void __launch_bounds__(mpf::NT, 2)
                     float u = AT(S_U2, lx, ly);
                     if (FCT) {
                         if (u > 0.0f)
-                            u = fmin_(fmin_(1.0f, AT(S_BXI, lx, ly)), AT(S_BXO, lx - 1, ly)) * u;
+                            u = fminf(fminf(1.0f, AT(S_BXI, lx, ly)), AT(S_BXO, lx - 1, ly)) * u;
                         else if (u < 0.0f)
-                            u = fmin_(fmin_(1.0f, AT(S_BXI, lx - 1, ly)), AT(S_BXO, lx, ly)) * u;
+                            u = fminf(fminf(1.0f, AT(S_BXI, lx - 1, ly)), AT(S_BXO, lx, ly)) * u;
                     }
                     u2l[ly * PW + lx] = u;
                 }
@@ -479,9 +488,9 @@ __global__ void __launch_bounds__(mpf::NT, 2)
                     float v = AT(S_V2, lx, ly);
                     if (FCT) {
                         if (v > 0.0f)
-                            v = fmin_(fmin_(1.0f, AT(S_BYI, lx, ly)), AT(S_BYO, lx, ly - 1)) * v;
+                            v = fminf(fminf(1.0f, AT(S_BYI, lx, ly)), AT(S_BYO, lx, ly - 1)) * v;
                         else if (v < 0.0f)
-                            v = fmin_(fmin_(1.0f, AT(S_BYI, lx, ly - 1)), AT(S_BYO, lx, ly)) * v;
+                            v = fminf(fminf(1.0f, AT(S_BYI, lx, ly - 1)), AT(S_BYO, lx, ly)) * v;
                     }
                     v2l[ly * PW + lx] = v;
                 }
@@ -492,9 +501,9 @@ __global__ void __launch_bounds__(mpf::NT, 2)
                 float w = r_w2[rr];
                 if (FCT && t >= 1) {
                     if (w > 0.0f)
-                        w = fmin_(fmin_(1.0f, n_bzi[rr]), r_bzo[rr]) * w;
+                        w = fminf(fminf(1.0f, n_bzi[rr]), r_bzo[rr]) * w;
                     else if (w < 0.0f)
-                        w = fmin_(fmin_(1.0f, r_bzi[rr]), n_bzo[rr]) * w;
+                        w = fminf(fminf(1.0f, r_bzi[rr]), n_bzo[rr]) * w;
                 }
                 n_w2l[rr] = w;
             }
@@ -515,24 +524,24 @@ __global__ void __launch_bounds__(mpf::NT, 2)
             for (int rr = 0; rr < RPW; rr++) {
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
                 const int i = i0 - 2 + lx, j = j0 - 2 + ly;
-                if (lane < TX && i <= nx - 2 && j <= ny - 2) {
+                if (lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
                     const float qc = AT(sQL, lx, ly);
                     const float fe = flux1(qc, AT(sQL, lx + 1, ly), u2l[ly * PW + lx + 1]);
                     const float fw = flux1(AT(sQL, lx - 1, ly), qc, u2l[ly * PW + lx]);
                     const float f3 = flux1(qc, AT(sQL, lx, ly + 1), v2l[(ly + 1) * PW + lx]);
                     const float f4 = flux1(AT(sQL, lx, ly - 1), qc, v2l[ly * PW + lx]);
-                    float val = qc - ((fe - fw) + (f3 - f4)) / r_G[rr];
+                    float val = qc - div0((fe - fw) + (f3 - f4), r_G[rr]);
                     const float wtop = n_w2l[rr], wbot = r_w2l[rr];
                     if (L > 0 && L < nz - 1) {
                         const float f5t = flux1(qc, AT(sQc, lx, ly), wtop);
                         const float f5b = flux1(r_q1dd[rr], qc, wbot);
-                        val = val - (f5t - f5b) / r_DJR[rr];
+                        val = val - div0(f5t - f5b, r_DJR[rr]);
                     } else if (L == 0) {
                         const float f5t = flux1(qc, AT(sQc, lx, ly), wtop);
-                        val = val - f5t / r_DJR[rr];
+                        val = val - div0(f5t, r_DJR[rr]);
                     } else {
                         const float f5b = flux1(r_q1dd[rr], qc, wbot);
-                        val = val - (qc * wtop - f5b) / r_DJR[rr];
+                        val = val - div0(qc * wtop - f5b, r_DJR[rr]);
                     }
                     outg[ix(g, i, L, j)] = val;
                 }
@@ -544,7 +553,7 @@ __global__ void __launch_bounds__(mpf::NT, 2)
 #pragma unroll
             for (int rr = 0; rr < RPW; rr++) {
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
-                const int i = min(i0 - 2 + lx, nx - 1), j = min(j0 - 2 + ly, ny - 1);
+                const int i = max(min(i0 - 2 + lx, nx - 1), 0), j = min(j0 - 2 + ly, ny - 1);
                 r_q1dd[rr] = r_q1dn[rr];
                 r_q1dn[rr] = AT(sQc, lx, ly);   // q1 at level t, "below" for level t+1
                 r_q0dn[rr] = AT(sQ0c, lx, ly);
@@ -563,7 +572,8 @@ __global__ void __launch_bounds__(mpf::NT, 2)
 
 inline bool fused_eligible(int order, int fct) { return order == 2 && (fct == 0 || fct == 1); }
 
-inline int mp_tiles_x(const Geo &g) { return (g.nx - 2 + mpf::TX - 1) / mpf::TX; }
+// tile tx covers output columns [TX*tx-2, TX*tx+TX-2); the last must reach nx-2
+inline int mp_tiles_x(const Geo &g) { return g.nx / mpf::TX + 1; }
 inline int mp_tiles_y(const Geo &g) { return (g.ny - 2 + mpf::TY - 1) / mpf::TY; }
 
 // Debug check (parameters%debug): flags any interior cell whose donor-cell
@@ -581,10 +591,10 @@ __global__ void k_courant(Geo g, const float *__restrict__ Um, const float *__re
     if (j >= g.ny || i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) return;
     size_t c = ix(g, i, k, j), sy = (size_t)g.P * g.nz, sz = (size_t)g.P;
     float r = use_rho ? rho[c] : 1.0f;
-    float h = (fmax_(0.0f, Um[c + 1]) - fmin_(0.0f, Um[c]) + fmax_(0.0f, Vm[c + sy]) - fmin_(0.0f, Vm[c])) /
+    float h = (fmaxf(0.0f, Um[c + 1]) - fminf(0.0f, Um[c]) + fmaxf(0.0f, Vm[c + sy]) - fminf(0.0f, Vm[c])) /
               (jaco[c] * r);
     float wb = k > 0 ? Wm[c - sz] : 0.0f;
-    float v = (fmax_(0.0f, Wm[c]) - fmin_(0.0f, wb)) / (dz[c] * jaco[c] * r);
+    float v = (fmaxf(0.0f, Wm[c]) - fminf(0.0f, wb)) / (dz[c] * jaco[c] * r);
     if (!(h + v <= 1.0f)) atomicExch(flag, 1);
 }
 

@@ -212,6 +212,8 @@ def build_case(nx, ny, nz, dx, dz_levels, terrain, U, V=0.0, mountain_N=None, wi
                species=("qv",), seed=0, dt=20.0, qv_noise=0.01) -> Case:
     rng = np.random.default_rng(seed)
     dz_levels = np.asarray(dz_levels, F32)
+    if float(terrain.max()) >= float(dz_levels.sum()):
+        raise ValueError("terrain reaches the model lid: the terrain-following jacobian would be <= 0")
     jac, ju, jv, jw, adz, z = vertical_grid(terrain, dz_levels, nx, ny)
     u = np.full((ny, nz, nx + 1), U, F32)
     v = np.full((ny + 1, nz, nx), V, F32)
@@ -247,7 +249,8 @@ def config2(seed: int = 0, nx: int = 512, ny: int = 512, nz: int = 40) -> Case:
     rng = np.random.default_rng(seed + 1000)
     dx = 1000.0
     terrain = fractal_terrain(nx, ny, dx, 600.0, 3000.0, rng)
-    return build_case(nx, ny, nz, dx, [500.0] * nz, terrain, U=15.0, mountain_N=0.01, wind_noise=0.05,
+    dzl = max(500.0, 20000.0 / nz)      # 500 m levels at nz=40; the lid stays at >= 20 km for small nz
+    return build_case(nx, ny, nz, dx, [dzl] * nz, terrain, U=15.0, mountain_N=0.01, wind_noise=0.05,
                       species=ALL12, seed=seed, dt=4.0)
 
 
