@@ -43,7 +43,10 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="full_species", choices=["full_species", "plain_c1", "mid_species"])
+    p.add_argument("--workload", default="full_species",
+                   choices=["full_species", "plain_c1", "mid_species", "ensemble"])
+    p.add_argument("--members", type=int, default=64, help="ensemble size (ensemble workload)")
+    p.add_argument("--tile-shape", type=int, default=1, help="fused-kernel tile shape 0..3 (8/16/24/32 rows)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
     p.add_argument("--quick", action="store_true",
@@ -320,10 +323,195 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------ ensemble
+ENSEMBLE_DESC = ("batched uneven ensemble: 64 independent domains, nx,ny ~ U[64,384], nz ~ U[20,50], "
+                 "12 fields each, dt 20 s, one graph launch per step vs 64 plain launches")
+
+
+def _member(args):
+    seed, nx, ny, nz = args
+    from hicar_b200 import synth
+    return synth.ensemble_member(seed, nx, ny, nz)
+
+
+def make_ensemble(n: int, seed: int):
+    """The members of the uneven ensemble, generated in parallel (spawned
+    workers, so no CUDA state is inherited)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from hicar_b200 import synth
+    shapes = synth.ensemble_shapes(n, seed)
+    jobs = [(seed * 1000 + i, nx, ny, nz) for i, (nx, ny, nz) in enumerate(shapes)]
+    workers = max(1, min(len(jobs), (os.cpu_count() or 2) - 1))
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_member, jobs))
+
+
+def run_ensemble(args):
+    import torch
+
+    from hicar_b200 import _lib as L, roofline
+    from hicar_b200.advection import Domain, Options, adv_init
+    from hicar_b200.batch import Batch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cases = make_ensemble(args.members, 7 + rank)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    lib = L.load()
+    opts = Options()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    doms = []
+    for c in cases:
+        d = Domain.from_case(c, device=local)
+        for k, q in c.species.items():
+            d.set_forcing(k, q, None)           # fixed inflow boundaries
+        adv_init(d, opts)
+        L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
+        doms.append(d)
+    cs_step = sum(c.cells() * len(c.species) for c in cases)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, steps):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- plain: one domain per launch sequence, members one after another
+    def plain_step():
+        for d, c in zip(doms, cases):
+            L.check(lib.icar_adv_step(d.handle, C.c_double(c.dt), 0), d.handle)
+
+    for _ in range(2):
+        plain_step()
+    plain_steps = max(3, args.steps // 4)
+    plain_ms = timed(plain_step, plain_steps)
+    plain_value = cs_step * plain_steps * world / (plain_ms / 1e3)
+
+    # ---- batched: every member in one graph launch per step
+    b = Batch(device=local)
+    b.set_stream(stream.cuda_stream)
+    b.set_tile_shape(args.tile_shape)
+    for d, c in zip(doms, cases):
+        b.add(d, c.dt)
+    for _ in range(args.warmup):
+        b.step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    b.profile(True)
+    ms = timed(b.step, args.steps)
+    clk = clocks.stop()
+    prof = b.profile_read()
+    b.profile(False)
+    value = cs_step * args.steps * world / (ms / 1e3)
+    bytes_step = sum(c.cells() * (8 * len(c.species) + 32) for c in cases)
+    peak, kind = roofline.hbm_peak()
+    step_ms = prof["ms"] / max(prof["steps"], 1)
+    achieved = bytes_step / (step_ms / 1e3) / 1e9
+    rl = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+          "traffic": None, "peak_kind": kind, "algorithmic_bytes_per_launch": bytes_step, "launch_ms": step_ms,
+          "bytes_model": "8 + 32/S B per cell-species; one launch = one batched step (graph)"}
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "quick": True, "plain_value": plain_value,
+                              "ms_per_step": ms / args.steps, "roofline": rl}), flush=True)
+        b.close()
+        for d in doms:
+            d.close()
+        return
+
+    # ---- end to end: host buffers in and out of every member every step
+    host = [{k: torch.from_numpy(v.copy()).pin_memory() for k, v in c.species.items()} for c in cases]
+
+    def e2e_step():
+        for d, hb in zip(doms, host):
+            for k, tns in hb.items():
+                L.check(lib.icar_adv_set_field(d.handle, L.SPECIES_IDS[k], C.c_void_p(tns.data_ptr()), None), d.handle)
+        b.step()
+        for d, hb in zip(doms, host):
+            for k, tns in hb.items():
+                L.check(lib.icar_adv_get_field(d.handle, L.SPECIES_IDS[k], C.c_void_p(tns.data_ptr()), None), d.handle)
+
+    e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    e2e_steps = 3
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = cs_step * e2e_steps * world / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        big = max(cases, key=lambda c: c.cells())
+        rate, el = cpu_rate(big.copy(), 2, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"largest member {big.nx}x{big.ny}x{big.nz}, 12 fields, 2 steps, {el:.1f} s "
+                         f"(C restatement, OpenMP)"}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": ENSEMBLE_DESC, "members": len(cases), "cell_species_per_step": cs_step,
+                       "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
+                       "tile_shape_rows": [8, 16, 24, 32][args.tile_shape],
+                       "l2": "inputs larger than L2 (~6 GB of species per step)",
+                       "parallelism": f"replicas x{world}"},
+            "plain": {"value": plain_value, "steps": plain_steps, "ms_per_step": plain_ms / plain_steps,
+                      "launches_per_step": sum(len(c.species) + 3 for c in cases)},
+            "batched_over_plain": value / plain_value,
+            "roofline": rl,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": cs_step * 4, "d2h_bytes_per_step": cs_step * 4,
+                    "steps": e2e_steps},
+            "gpu_launches": int(prof["kernels_per_step"] * prof["steps"]),
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    b.close()
+    for d in doms:
+        d.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
     else:
         run_b200(args)
 

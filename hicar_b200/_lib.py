@@ -81,6 +81,21 @@ _PROTOS = {
     "icar_adv_last_error": (C.c_char_p, [C.c_void_p]),
     "icar_adv_set_path": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "icar_adv_batch_destroy": (C.c_int, [C.c_void_p]),
+    "icar_adv_batch_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "icar_adv_batch_remove": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "icar_adv_batch_set_dt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "icar_adv_batch_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_batch_step": (C.c_int, [C.c_void_p]),
+    "icar_adv_batch_sync": (C.c_int, [C.c_void_p]),
+    "icar_adv_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "icar_adv_batch_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_batch_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                              C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "icar_adv_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "icar_adv_tile_shapes": (C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "icar_adv_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                         C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }

@@ -1,0 +1,260 @@
+// Batched form: many independent domains (ensemble members or served
+// requests) of uneven nx x ny x nz advance together.  One step is five
+// launches whatever the number of members, captured once in a CUDA graph:
+//   k_batch_forcing  relaxation-zone update of every forced species
+//   k_batch_prep     species-independent per-step fields of every member
+//   k_batch_upwind   donor-cell pass of every species of every member
+//   (counter reset)
+//   k_batch_corr     persistent CTAs pulling (member, species, tile) items
+//                    from a cost-sorted work list with an atomic counter and
+//                    running the fused z-march of mpdata_fused.cuh on each.
+// Member data lives in a device table (BatchMember); the simple kernels map
+// their flat block index to a member by binary search over per-member block
+// prefix sums.
+#pragma once
+#include "boundary_kernels.cuh"
+#include "common.cuh"
+#include "mpdata_fused.cuh"
+
+namespace icar {
+
+constexpr int BATCH_MAX_SPECIES = 32;
+
+struct BatchMember {
+    Geo g;
+    float dx, dt;
+    double dtd;
+    int S, adv_den, nzone, pad;
+    const float *u, *v, *w, *rho, *jac, *ju, *jv, *jw, *dz;
+    float *Um, *Vm, *Wm, *Gc, *DJR, *Wp;
+    const float *filter;
+    const int *zone;
+    const float *q0[BATCH_MAX_SPECIES];
+    float *q1[BATCH_MAX_SPECIES];
+    float *out[BATCH_MAX_SPECIES];
+    float *forcing[BATCH_MAX_SPECIES];
+    const float *dqdt[BATCH_MAX_SPECIES];
+};
+
+// index of the last prefix entry <= b (prefix[0] = 0, prefix[n] = total)
+__device__ __forceinline__ int find_owner(const int *__restrict__ prefix, int n, int b)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// pairs[p] = (member, species) of the p-th forced species; prefix over their
+// blocks of ceil(nzone*nz/256).
+__global__ void k_batch_forcing(const BatchMember *__restrict__ mem, const int *__restrict__ prefix,
+                                const int2 *__restrict__ pairs, int npairs)
+{
+    const int p = find_owner(prefix, npairs, blockIdx.x);
+    const int2 ms = pairs[p];
+    const BatchMember &m = mem[ms.x];
+    const size_t t = (size_t)(blockIdx.x - prefix[p]) * blockDim.x + threadIdx.x;
+    const Geo g = m.g;
+    if (t >= (size_t)m.nzone * g.nz) return;
+    const int z = (int)(t % (size_t)m.nzone);
+    const int k = (int)(t / (size_t)m.nzone);
+    const int packed = m.zone[z];
+    const int i = packed % g.nx, j = packed / g.nx;
+    const size_t c = ix(g, i, k, j);
+    float *q = const_cast<float *>(m.q0[ms.y]);
+    float *fo = m.forcing[ms.y];
+    const float fnew = (float)((double)fo[c] + (double)m.dqdt[ms.y][c] * m.dtd);
+    fo[c] = fnew;
+    const float flt = m.filter[packed];
+    if (flt == 1.0f)
+        q[c] = fnew;
+    else if (flt < 1.0f)
+        q[c] = (float)((double)q[c] + ((double)flt * m.dtd / 3600.0) * (double)(fnew - q[c]));
+}
+
+// prefix over members of ceil((nx+1)*nz*(ny+1)/256) blocks
+__global__ void k_batch_prep(const BatchMember *__restrict__ mem, const int *__restrict__ prefix, int nmem)
+{
+    const int mi = find_owner(prefix, nmem, blockIdx.x);
+    const BatchMember &m = mem[mi];
+    const Geo g = m.g;
+    const size_t t = (size_t)(blockIdx.x - prefix[mi]) * blockDim.x + threadIdx.x;
+    const int ni = g.nx + 1, nk = g.nz, nj = g.ny + 1;
+    const int i = (int)(t % (size_t)ni);
+    const size_t rest = t / (size_t)ni;
+    const int k = (int)(rest % (size_t)nk);
+    const int j = (int)(rest / (size_t)nk);
+    if (j >= nj) return;
+    const int adv_den = m.adv_den;
+    const float dt = m.dt, dx = m.dx;
+    if (j < g.ny) {
+        size_t c = ix(g, i, k, j);
+        if (i >= 1 && i <= g.nx - 1) {
+            float rr = adv_den ? m.rho[c] : 1.0f;
+            float rl = adv_den ? m.rho[c - 1] : 1.0f;
+            m.Um[c] = m.u[c] * dt * (rr + rl) * 0.5f * m.ju[c] / dx;
+        } else {
+            m.Um[c] = 0.0f;
+        }
+        if (i < g.nx) {
+            float r0 = adv_den ? m.rho[c] : 1.0f;
+            float wm;
+            if (k < g.nz - 1) {
+                float r1 = adv_den ? m.rho[ix(g, i, k + 1, j)] : 1.0f;
+                wm = m.w[c] * dt * m.jw[c] * (r1 + r0) * 0.5f;
+            } else {
+                wm = m.w[c] * dt * m.jw[c] * r0;
+            }
+            m.Wm[c] = wm;
+            const float d = m.dz[c], jj = m.jac[c], rh = m.rho[c];
+            m.Gc[c] = jj * rh;
+            m.DJR[c] = d * jj * rh;
+            m.Wp[c] = wm / d;
+        }
+    }
+    if (i < g.nx) {
+        size_t c = ix(g, i, k, j);
+        if (j >= 1 && j <= g.ny - 1) {
+            float rr = adv_den ? m.rho[c] : 1.0f;
+            float rl = adv_den ? m.rho[ix(g, i, k, j - 1)] : 1.0f;
+            m.Vm[c] = m.v[c] * dt * (rr + rl) * 0.5f * m.jv[c] / dx;
+        } else {
+            m.Vm[c] = 0.0f;
+        }
+    }
+}
+
+// prefix over members of S * ceil(nx*nz*ny/256) blocks; nblk[m] = blocks per species
+__global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix,
+                               const int *__restrict__ nblk, int nmem)
+{
+    const int mi = find_owner(prefix, nmem, blockIdx.x);
+    const BatchMember &m = mem[mi];
+    const Geo g = m.g;
+    const int local = blockIdx.x - prefix[mi];
+    const int s = local / nblk[mi];
+    const size_t t = (size_t)(local - s * nblk[mi]) * blockDim.x + threadIdx.x;
+    const int i = (int)(t % (size_t)g.nx);
+    const size_t rest = t / (size_t)g.nx;
+    const int k = (int)(rest % (size_t)g.nz);
+    const int j = (int)(rest / (size_t)g.nz);
+    if (j >= g.ny) return;
+    const float *__restrict__ qin = m.q0[s];
+    const size_t c = ix(g, i, k, j);
+    const float q0 = qin[c];
+    if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) {
+        m.q1[s][c] = q0;
+        m.out[s][c] = q0;
+        return;
+    }
+    const size_t sy = (size_t)g.P * g.nz, sz = (size_t)g.P;
+    const float *__restrict__ U = m.Um, *__restrict__ V = m.Vm, *__restrict__ W = m.Wm;
+    float fe = flux1(q0, qin[c + 1], U[c + 1]);
+    float fw = flux1(qin[c - 1], q0, U[c]);
+    float f3 = flux1(q0, qin[c + sy], V[c + sy]);
+    float f4 = flux1(qin[c - sy], q0, V[c]);
+    float val = q0 - ((fe - fw) + (f3 - f4)) / m.Gc[c];
+    const float djr = m.DJR[c];
+    if (k > 0 && k < g.nz - 1) {
+        float f5t = flux1(q0, qin[c + sz], W[c]);
+        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
+        val = val - (f5t - f5b) / djr;
+    } else if (k == 0) {
+        float f5t = flux1(q0, qin[c + sz], W[c]);
+        val = val - f5t / djr;
+    } else {
+        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
+        val = val - (q0 * W[c] - f5b) / djr;
+    }
+    m.q1[s][c] = val;
+}
+
+// Persistent correction kernel: items are (member, species, i0, j0).
+template <bool FCT, class SH>
+__global__ void __launch_bounds__(SH::NT, (SH::NT <= 128 ? 5 : 3))
+    k_batch_corr(const BatchMember *__restrict__ mem, const int4 *__restrict__ items, int n_items,
+                 int *__restrict__ counter)
+{
+    extern __shared__ float4 sm4[];
+    __shared__ int next;
+    float *sm = reinterpret_cast<float *>(sm4);
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = next;
+        __syncthreads();
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const BatchMember &m = mem[w.x];
+        mp_corr_tile<FCT, SH>(sm, m.g, m.q0[w.y], m.q1[w.y], m.out[w.y], w.z, w.w, m.Um, m.Vm, m.Wp, m.Gc,
+                              m.DJR, m.dz);
+    }
+}
+
+template <class SH>
+inline cudaError_t batch_corr_attr()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_batch_corr<true, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mpf::smem_bytes<SH>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_corr<false, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mpf::smem_bytes<SH>());
+    return e;
+}
+
+inline cudaError_t batch_setup()
+{
+    cudaError_t e = batch_corr_attr<MpShape8>();
+    if (e == cudaSuccess) e = batch_corr_attr<MpShape16>();
+    if (e == cudaSuccess) e = batch_corr_attr<MpShape24>();
+    if (e == cudaSuccess) e = batch_corr_attr<MpShape32>();
+    return e;
+}
+
+// CTAs of the persistent kernel that fit on the device at once.
+template <class SH>
+inline int batch_corr_ctas(int fct, int nsm)
+{
+    int per = 0;
+    if (fct)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_corr<true, SH>, SH::NT, mpf::smem_bytes<SH>());
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_corr<false, SH>, SH::NT, mpf::smem_bytes<SH>());
+    return (per > 0 ? per : 1) * nsm;
+}
+
+template <class SH>
+inline void batch_corr_launch_t(cudaStream_t st, int ctas, int fct, const BatchMember *mem, const int4 *items,
+                                int n, int *counter)
+{
+    if (fct)
+        k_batch_corr<true, SH><<<ctas, SH::NT, mpf::smem_bytes<SH>(), st>>>(mem, items, n, counter);
+    else
+        k_batch_corr<false, SH><<<ctas, SH::NT, mpf::smem_bytes<SH>(), st>>>(mem, items, n, counter);
+}
+
+inline int batch_corr_max_ctas(int shape, int fct, int nsm)
+{
+    switch (shape) {
+    case 0: return batch_corr_ctas<MpShape8>(fct, nsm);
+    case 2: return batch_corr_ctas<MpShape24>(fct, nsm);
+    case 3: return batch_corr_ctas<MpShape32>(fct, nsm);
+    default: return batch_corr_ctas<MpShape16>(fct, nsm);
+    }
+}
+
+inline void batch_corr_launch(cudaStream_t st, int shape, int ctas, int fct, const BatchMember *mem,
+                              const int4 *items, int n, int *counter)
+{
+    switch (shape) {
+    case 0: batch_corr_launch_t<MpShape8>(st, ctas, fct, mem, items, n, counter); break;
+    case 2: batch_corr_launch_t<MpShape24>(st, ctas, fct, mem, items, n, counter); break;
+    case 3: batch_corr_launch_t<MpShape32>(st, ctas, fct, mem, items, n, counter); break;
+    default: batch_corr_launch_t<MpShape16>(st, ctas, fct, mem, items, n, counter); break;
+    }
+}
+
+}  // namespace icar

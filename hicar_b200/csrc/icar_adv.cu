@@ -22,6 +22,7 @@
 #include "mpdata_fused.cuh"
 #include "mpdata_kernels.cuh"
 #include "std_kernels.cuh"
+#include "batch_kernels.cuh"
 
 using icar::Geo;
 
@@ -65,12 +66,14 @@ struct icar_adv_domain {
     std::vector<DevBuf> qn, q1s;               // fused path: next state and pass-1 result per species
     bool fused_ready = false;
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
-    int path = 0;  // 0 = fused MPDATA kernel when eligible, 1 = staged kernels
+    int path = 0;      // 0 = fused MPDATA kernel when eligible, 1 = staged kernels
+    int mp_shape = 1;  // tile shape of the fused correction kernel (icar::mp_shape_ty)
     // diagnostics: launch counter and optional event timing of the species kernels
     int64_t launches = 0;
     int64_t timed_launches = 0;
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    icar_adv_batch *batch = nullptr;  // batch this domain is a member of, if any
     std::string err;
 };
 
@@ -272,6 +275,9 @@ int upload_filter(icar_adv_t *h)
     return ICAR_ADV_OK;
 }
 
+// A member's forcing buffers changed: its batch must rebuild tables and graphs.
+void batch_fields_changed(icar_adv_batch *b);
+
 // Resolve a field id to its device buffer, extents and presence flag.
 struct FieldRef {
     DevBuf *buf = nullptr;
@@ -317,6 +323,7 @@ int resolve(icar_adv_t *h, int field, FieldRef &r)
     if (fo) { int e = alloc(h, h->forcing[s], h->n_cell); if (e) return e; r.buf = &h->forcing[s]; }
     else if (dq) { int e = alloc(h, h->dqdt[s], h->n_cell); if (e) return e; r.buf = &h->dqdt[s]; }
     else r.buf = &h->q[s];
+    if ((fo || dq) && h->batch) batch_fields_changed(h->batch);
     return ICAR_ADV_OK;
 }
 
@@ -523,9 +530,8 @@ int std_advect3d(icar_adv_t *h, const float *qf, const float *qold, float *qout,
 
 // Fused MPDATA (order 2): prep -> pass 1 for all species -> fused
 // pseudo-velocity/FCT/corrective pass for all species, then swap buffers.
-int mpdata_fused_step(icar_adv_t *h, float dt)
+int ensure_fused(icar_adv_t *h)
 {
-    const Geo &g = h->g;
     const int S = h->desc.n_species;
     int e;
     if (!h->fused_ready) {
@@ -535,14 +541,19 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
             return e;
         for (int s = 0; s < S; s++)
             if ((e = alloc(h, h->qn[s], h->n_cell)) || (e = alloc(h, h->q1s[s], h->n_cell))) return e;
-        cudaError_t ce = cudaFuncSetAttribute(icar::k_mp_corr<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)icar::mpf::SMEM);
-        if (ce == cudaSuccess)
-            ce = cudaFuncSetAttribute(icar::k_mp_corr<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)icar::mpf::SMEM);
+        cudaError_t ce = icar::mp_corr_setup();
         if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaFuncSetAttribute: %s", cudaGetErrorString(ce));
         h->fused_ready = true;
     }
+    return ICAR_ADV_OK;
+}
+
+int mpdata_fused_step(icar_adv_t *h, float dt)
+{
+    const Geo &g = h->g;
+    const int S = h->desc.n_species;
+    int e = ensure_fused(h);
+    if (e) return e;
     const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
     icar::k_mp_prep<<<blocks_for(nf, 256), 256, 0, h->stream>>>(
         g, h->desc.dx, dt, h->opts.advect_density, h->u.p, h->v.p, h->w.p, h->rho.p, h->jac.p, h->jac_u.p,
@@ -560,14 +571,8 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
     if (S > 0) {
         dim3 gu(blocks_for(nc, 256), S);
         icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p, h->DJR.p);
-        const int tx = icar::mp_tiles_x(g), ty = icar::mp_tiles_y(g);
-        const unsigned nblk = (unsigned)(tx * ty * S);
-        if (h->opts.mpdata_fct)
-            icar::k_mp_corr<true><<<nblk, icar::mpf::NT, icar::mpf::SMEM, h->stream>>>(
-                g, sp, S, tx, h->Um.p, h->Vm.p, h->Wp.p, h->Gc.p, h->DJR.p, h->dz.p);
-        else
-            icar::k_mp_corr<false><<<nblk, icar::mpf::NT, icar::mpf::SMEM, h->stream>>>(
-                g, sp, S, tx, h->Um.p, h->Vm.p, h->Wp.p, h->Gc.p, h->DJR.p, h->dz.p);
+        icar::mp_corr_launch(h->stream, h->mp_shape, g, sp, S, h->opts.mpdata_fct, h->Um.p, h->Vm.p, h->Wp.p,
+                             h->Gc.p, h->DJR.p, h->dz.p);
     }
     e = check_launch(h, "fused MPDATA kernels", S > 0 ? 3 : 1);
     if (e) return e;
@@ -761,9 +766,12 @@ int icar_adv_create(const icar_adv_desc *desc, const icar_adv_opts *opts, icar_a
     return ICAR_ADV_OK;
 }
 
+int icar_adv_batch_remove(icar_adv_batch_t *b, icar_adv_t *member);
+
 int icar_adv_destroy(icar_adv_t *h)
 {
     if (!h) return ICAR_ADV_OK;
+    if (h->batch) icar_adv_batch_remove(h->batch, h);
     cudaSetDevice(h->desc.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
@@ -836,6 +844,7 @@ int icar_adv_get_field_device(icar_adv_t *h, int32_t field, float *dev) { return
 int icar_adv_advect(icar_adv_t *h, float dt)
 {
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (h->batch) return fail(h, ICAR_ADV_BAD_ARG, "domain is a batch member: step it with icar_adv_batch_step");
     cudaSetDevice(h->desc.device);
     return advect_impl(h, dt);
 }
@@ -843,6 +852,7 @@ int icar_adv_advect(icar_adv_t *h, float dt)
 int icar_adv_apply_forcing(icar_adv_t *h, double dt_seconds)
 {
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (h->batch) return fail(h, ICAR_ADV_BAD_ARG, "domain is a batch member: step it with icar_adv_batch_step");
     cudaSetDevice(h->desc.device);
     if (!std::isfinite(dt_seconds)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite");
     if (h->nzone == 0) return ICAR_ADV_OK;
@@ -945,6 +955,23 @@ int icar_adv_profile_read(icar_adv_t *h, double *species_kernel_ms, int64_t *spe
     return ICAR_ADV_OK;
 }
 
+int icar_adv_set_tile_shape(icar_adv_t *h, int32_t shape)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (shape < 0 || shape >= icar::MP_NSHAPES) return fail(h, ICAR_ADV_BAD_ARG, "tile shape %d out of range", shape);
+    h->mp_shape = shape;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_tile_shapes(int32_t *n_shapes, int32_t *rows)
+{
+    if (!n_shapes) return fail(nullptr, ICAR_ADV_BAD_ARG, "NULL argument");
+    if (rows && *n_shapes >= icar::MP_NSHAPES)
+        for (int i = 0; i < icar::MP_NSHAPES; i++) rows[i] = icar::mp_shape_ty(i);
+    *n_shapes = icar::MP_NSHAPES;
+    return ICAR_ADV_OK;
+}
+
 // Internal selector used by the tests and the benchmark to run the staged
 // kernels instead of the fused one (0 = fused when eligible, 1 = staged).
 int icar_adv_set_path(icar_adv_t *h, int32_t path)
@@ -953,5 +980,447 @@ int icar_adv_set_path(icar_adv_t *h, int32_t path)
     h->path = path;
     return ICAR_ADV_OK;
 }
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched form
+// ===========================================================================
+struct icar_adv_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int nsm = 0;
+    std::vector<icar_adv_t *> members;
+    std::vector<double> dts;
+    int shape = 1;
+    int fct = -1;
+    bool tables_dirty = true, graph_dirty = true;
+    int parity = 0;
+    // device tables and work lists
+    icar::BatchMember *d_mem[2] = {nullptr, nullptr};
+    size_t mem_cap = 0;
+    int *d_ints = nullptr;   // prep prefix | upwind prefix | upwind nblk | forcing prefix | counter
+    size_t ints_cap = 0;
+    int2 *d_pairs = nullptr;
+    size_t pairs_cap = 0;
+    int4 *d_items = nullptr;
+    size_t items_cap = 0;
+    int n_prep = 0, n_up = 0, n_force = 0, n_pairs = 0, n_items = 0, ctas = 0;
+    size_t off_up = 0, off_nblk = 0, off_f = 0, off_counter = 0;
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    int64_t steps = 0;
+    std::string err;
+};
+
+namespace {
+
+void batch_fields_changed(icar_adv_batch *b) { b->tables_dirty = b->graph_dirty = true; }
+
+int bfail(icar_adv_batch_t *b, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (b)
+        b->err = buf;
+    else
+        g_create_error = buf;
+    return code;
+}
+
+#define BCUDA(b, call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return bfail((b), e_ == cudaErrorMemoryAllocation ? ICAR_ADV_OOM : ICAR_ADV_CUDA_ERROR, \
+                         "%s failed: %s", #call, cudaGetErrorString(e_));                           \
+    } while (0)
+
+template <class T>
+int grow(icar_adv_batch_t *b, T *&p, size_t &cap, size_t n)
+{
+    if (n <= cap && p) return ICAR_ADV_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    size_t c = std::max<size_t>(n, 16);
+    BCUDA(b, cudaMalloc(&p, c * sizeof(T)));
+    cap = c;
+    return ICAR_ADV_OK;
+}
+
+void drop_graphs(icar_adv_batch_t *b)
+{
+    for (int p = 0; p < 2; p++) {
+        if (b->exec[p]) cudaGraphExecDestroy(b->exec[p]);
+        if (b->graph[p]) cudaGraphDestroy(b->graph[p]);
+        b->exec[p] = nullptr;
+        b->graph[p] = nullptr;
+    }
+}
+
+void fill_member(icar::BatchMember &m, icar_adv_t *h, double dt, int parity)
+{
+    memset(&m, 0, sizeof(m));
+    m.g = h->g;
+    m.dx = h->desc.dx;
+    m.dt = (float)dt;
+    m.dtd = dt;
+    m.S = h->desc.n_species;
+    m.adv_den = h->opts.advect_density;
+    m.nzone = h->nzone;
+    m.u = h->u.p; m.v = h->v.p; m.w = h->w.p; m.rho = h->rho.p; m.jac = h->jac.p;
+    m.ju = h->jac_u.p; m.jv = h->jac_v.p; m.jw = h->jac_w.p; m.dz = h->dz.p;
+    m.Um = h->Um.p; m.Vm = h->Vm.p; m.Wm = h->Wm.p; m.Gc = h->Gc.p; m.DJR = h->DJR.p; m.Wp = h->Wp.p;
+    m.filter = h->filter_dev;
+    m.zone = h->zone_dev;
+    for (int s = 0; s < m.S; s++) {
+        // parity 0: current state in q, next in qn; parity 1 the other way round
+        float *cur = parity == 0 ? h->q[s].p : h->qn[s].p;
+        float *nxt = parity == 0 ? h->qn[s].p : h->q[s].p;
+        m.q0[s] = cur;
+        m.out[s] = nxt;
+        m.q1[s] = h->q1s[s].p;
+        m.forcing[s] = h->forcing[s].p;
+        m.dqdt[s] = h->dqdt[s].p;
+    }
+}
+
+// Rebuild the member tables (both buffer parities) and the work lists.
+int build_tables(icar_adv_batch_t *b)
+{
+    const int M = (int)b->members.size();
+    std::vector<icar::BatchMember> mem[2];
+    mem[0].resize(std::max(M, 1));
+    mem[1].resize(std::max(M, 1));
+    std::vector<int> prep(M + 1, 0), up(M + 1, 0), nblk(std::max(M, 1), 0), fpre(1, 0);
+    std::vector<int2> pairs;
+    std::vector<int4> items;
+    const int ty = icar::mp_shape_ty(b->shape);
+    for (int m = 0; m < M; m++) {
+        icar_adv_t *h = b->members[m];
+        // members' buffers hold "current" in q at the batch's parity 0
+        fill_member(mem[0][m], h, b->dts[m], b->parity == 0 ? 0 : 1);
+        fill_member(mem[1][m], h, b->dts[m], b->parity == 0 ? 1 : 0);
+        const Geo &g = h->g;
+        const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+        const size_t nc = (size_t)g.nx * g.nz * g.ny;
+        prep[m + 1] = prep[m] + (int)((nf + 255) / 256);
+        nblk[m] = (int)((nc + 255) / 256);
+        up[m + 1] = up[m] + nblk[m] * h->desc.n_species;
+        for (int s = 0; s < h->desc.n_species; s++) {
+            if (h->forcing[s].p && h->nzone > 0) {
+                pairs.push_back(make_int2(m, s));
+                fpre.push_back(fpre.back() + (int)(((size_t)h->nzone * g.nz + 255) / 256));
+            }
+        }
+        const int tx = icar::mp_tiles_x(g), tyn = icar::mp_tiles_y(g, ty);
+        for (int s = 0; s < h->desc.n_species; s++)
+            for (int a = 0; a < tyn; a++)
+                for (int c = 0; c < tx; c++)
+                    items.push_back(make_int4(m, s, c * icar::mpf::TX - 2, 1 + a * ty));
+    }
+    // longest columns first (cost ~ nz per tile), so the tail of the
+    // persistent launch is made of short items
+    std::stable_sort(items.begin(), items.end(), [&](const int4 &x, const int4 &y) {
+        return b->members[x.x]->g.nz > b->members[y.x]->g.nz;
+    });
+    b->n_prep = prep[M];
+    b->n_up = up[M];
+    b->n_pairs = (int)pairs.size();
+    b->n_force = fpre.back();
+    b->n_items = (int)items.size();
+    int e;
+    if ((size_t)std::max(M, 1) > b->mem_cap || !b->d_mem[0]) {
+        for (int p = 0; p < 2; p++) {
+            if (b->d_mem[p]) cudaFree(b->d_mem[p]);
+            b->d_mem[p] = nullptr;
+        }
+        b->mem_cap = 0;
+        const size_t cap = std::max<size_t>(M, 16);
+        for (int p = 0; p < 2; p++) BCUDA(b, cudaMalloc(&b->d_mem[p], cap * sizeof(icar::BatchMember)));
+        b->mem_cap = cap;
+    }
+    b->off_up = M + 1;
+    b->off_nblk = b->off_up + M + 1;
+    b->off_f = b->off_nblk + std::max(M, 1);
+    b->off_counter = b->off_f + fpre.size();
+    std::vector<int> ints(b->off_counter + 1, 0);
+    std::copy(prep.begin(), prep.end(), ints.begin());
+    std::copy(up.begin(), up.end(), ints.begin() + b->off_up);
+    std::copy(nblk.begin(), nblk.end(), ints.begin() + b->off_nblk);
+    std::copy(fpre.begin(), fpre.end(), ints.begin() + b->off_f);
+    if ((e = grow(b, b->d_ints, b->ints_cap, ints.size()))) return e;
+    if ((e = grow(b, b->d_pairs, b->pairs_cap, std::max<size_t>(pairs.size(), 1)))) return e;
+    if ((e = grow(b, b->d_items, b->items_cap, std::max<size_t>(items.size(), 1)))) return e;
+    BCUDA(b, cudaMemcpyAsync(b->d_mem[0], mem[0].data(), sizeof(icar::BatchMember) * std::max(M, 1),
+                             cudaMemcpyHostToDevice, b->stream));
+    BCUDA(b, cudaMemcpyAsync(b->d_mem[1], mem[1].data(), sizeof(icar::BatchMember) * std::max(M, 1),
+                             cudaMemcpyHostToDevice, b->stream));
+    BCUDA(b, cudaMemcpyAsync(b->d_ints, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice, b->stream));
+    if (!pairs.empty())
+        BCUDA(b, cudaMemcpyAsync(b->d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice,
+                                 b->stream));
+    if (!items.empty())
+        BCUDA(b, cudaMemcpyAsync(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice,
+                                 b->stream));
+    // the host vectors die here: finish the copies first
+    BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->ctas = std::min(std::max(b->n_items, 1), icar::batch_corr_max_ctas(b->shape, b->fct, b->nsm));
+    b->tables_dirty = false;
+    return ICAR_ADV_OK;
+}
+
+// Enqueue one batched step using the member table of the given parity.
+void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
+{
+    const icar::BatchMember *mem = b->d_mem[p];
+    const int M = (int)b->members.size();
+    if (b->n_force > 0)
+        icar::k_batch_forcing<<<b->n_force, 256, 0, st>>>(mem, b->d_ints + b->off_f, b->d_pairs, b->n_pairs);
+    if (b->n_prep > 0) icar::k_batch_prep<<<b->n_prep, 256, 0, st>>>(mem, b->d_ints, M);
+    if (b->n_up > 0)
+        icar::k_batch_upwind<<<b->n_up, 256, 0, st>>>(mem, b->d_ints + b->off_up, b->d_ints + b->off_nblk, M);
+    cudaMemsetAsync(b->d_ints + b->off_counter, 0, sizeof(int), st);
+    if (b->n_items > 0)
+        icar::batch_corr_launch(st, b->shape, b->ctas, b->fct, mem, b->d_items, b->n_items,
+                                b->d_ints + b->off_counter);
+}
+
+int build_graphs(icar_adv_batch_t *b)
+{
+    drop_graphs(b);
+    for (int p = 0; p < 2; p++) {
+        BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(b, p, b->stream);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph[p]);
+        if (e != cudaSuccess) return bfail(b, ICAR_ADV_CUDA_ERROR, "graph capture failed: %s", cudaGetErrorString(e));
+        BCUDA(b, cudaGraphInstantiate(&b->exec[p], b->graph[p], 0));
+    }
+    b->graph_dirty = false;
+    return ICAR_ADV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int icar_adv_batch_create(int32_t device, icar_adv_batch_t **out)
+{
+    if (!out) return bfail(nullptr, ICAR_ADV_BAD_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return bfail(nullptr, ICAR_ADV_CUDA_ERROR, "device %d not available", device);
+    cudaSetDevice(device);
+    icar_adv_batch_t *b = new icar_adv_batch();
+    b->device = device;
+    cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = icar::mp_corr_setup();
+    if (e == cudaSuccess) e = icar::batch_setup();
+    if (e != cudaSuccess) {
+        int code = bfail(nullptr, ICAR_ADV_CUDA_ERROR, "batch setup failed: %s", cudaGetErrorString(e));
+        if (b->stream) cudaStreamDestroy(b->stream);
+        delete b;
+        return code;
+    }
+    *out = b;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_add(icar_adv_batch_t *b, icar_adv_t *h, double dt_seconds)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    if (!h) return bfail(b, ICAR_ADV_BAD_ARG, "member is NULL");
+    if (h->batch) return bfail(b, ICAR_ADV_BAD_ARG, "domain already belongs to a batch");
+    if (h->desc.device != b->device) return bfail(b, ICAR_ADV_BAD_ARG, "member lives on another device");
+    if (h->opts.advection != ICAR_ADV_MPDATA || h->opts.rk3 || !icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct))
+        return bfail(b, ICAR_ADV_BAD_ARG, "batched members must use MPDATA order 2 (with or without FCT), no RK3");
+    if (b->fct >= 0 && b->fct != h->opts.mpdata_fct)
+        return bfail(b, ICAR_ADV_BAD_ARG, "all members of a batch share the MPDATA_FCT switch");
+    if (!(dt_seconds >= 0.0) || !std::isfinite(dt_seconds)) return bfail(b, ICAR_ADV_BAD_ARG, "dt must be finite, >= 0");
+    cudaSetDevice(b->device);
+    int e = ensure_ready(h);
+    if (e) return bfail(b, e, "member not ready: %s", h->err.c_str());
+    e = ensure_fused(h);
+    if (e) return bfail(b, e, "member scratch: %s", h->err.c_str());
+    // order the member's pending work before the batch's, then share the stream
+    cudaStreamSynchronize(h->stream);
+    for (int s = 0; s < h->desc.n_species; s++)
+        if (h->forcing[s].p && !h->dqdt[s].p) {
+            e = alloc(h, h->dqdt[s], h->n_cell);
+            if (e) return bfail(b, e, "%s", h->err.c_str());
+        }
+    cudaStreamSynchronize(h->stream);
+    h->stream = b->stream;
+    h->batch = b;
+    b->fct = h->opts.mpdata_fct;
+    b->members.push_back(h);
+    b->dts.push_back(dt_seconds);
+    b->tables_dirty = b->graph_dirty = true;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_remove(icar_adv_batch_t *b, icar_adv_t *h)
+{
+    if (!b || !h) return bfail(b, ICAR_ADV_BAD_ARG, "NULL argument");
+    auto it = std::find(b->members.begin(), b->members.end(), h);
+    if (it == b->members.end()) return bfail(b, ICAR_ADV_BAD_ARG, "domain is not a member of this batch");
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->dts.erase(b->dts.begin() + (it - b->members.begin()));
+    b->members.erase(it);
+    h->batch = nullptr;
+    h->stream = h->own_stream;
+    if (b->members.empty()) b->fct = -1;
+    b->tables_dirty = b->graph_dirty = true;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_set_dt(icar_adv_batch_t *b, icar_adv_t *h, double dt_seconds)
+{
+    if (!b || !h) return bfail(b, ICAR_ADV_BAD_ARG, "NULL argument");
+    auto it = std::find(b->members.begin(), b->members.end(), h);
+    if (it == b->members.end()) return bfail(b, ICAR_ADV_BAD_ARG, "domain is not a member of this batch");
+    if (!(dt_seconds >= 0.0) || !std::isfinite(dt_seconds)) return bfail(b, ICAR_ADV_BAD_ARG, "dt must be finite, >= 0");
+    b->dts[it - b->members.begin()] = dt_seconds;
+    b->tables_dirty = true;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_set_tile_shape(icar_adv_batch_t *b, int32_t shape)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    if (shape < 0 || shape >= icar::MP_NSHAPES) return bfail(b, ICAR_ADV_BAD_ARG, "tile shape out of range");
+    if (shape != b->shape) {
+        b->shape = shape;
+        b->tables_dirty = b->graph_dirty = true;
+    }
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_step(icar_adv_batch_t *b)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    cudaSetDevice(b->device);
+    if (b->members.empty()) return ICAR_ADV_OK;
+    int e;
+    if (b->tables_dirty) {
+        // tables are written relative to the current parity, so rebuild from parity 0
+        b->parity = 0;
+        if ((e = build_tables(b))) return e;
+        b->graph_dirty = true;
+    }
+    if (b->graph_dirty && (e = build_graphs(b))) return e;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (b->profiling) {
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, b->stream);
+    }
+    BCUDA(b, cudaGraphLaunch(b->exec[b->parity], b->stream));
+    if (b->profiling) {
+        cudaEventRecord(ev1, b->stream);
+        b->events.emplace_back(ev0, ev1);
+    }
+    b->steps++;
+    b->parity ^= 1;
+    // the members' "current" buffers are now the ones just written
+    for (icar_adv_t *h : b->members)
+        for (int s = 0; s < h->desc.n_species; s++) std::swap(h->q[s], h->qn[s]);
+    // keep the tables consistent with the swapped member buffers: parity p's
+    // table reads q (current) when p == parity, which holds by construction
+    // of build_tables (table[0] read q at parity 0, table[1] read qn) as the
+    // buffers and the parity flip together.
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_sync(icar_adv_batch_t *b)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    cudaSetDevice(b->device);
+    BCUDA(b, cudaStreamSynchronize(b->stream));
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_set_stream(icar_adv_batch_t *b, void *cuda_stream)
+{
+    if (!b || !cuda_stream) return bfail(b, ICAR_ADV_BAD_ARG, "batch or stream is NULL");
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->stream = (cudaStream_t)cuda_stream;
+    for (icar_adv_t *h : b->members) h->stream = b->stream;
+    b->graph_dirty = true;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_profile(icar_adv_batch_t *b, int32_t enable)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    for (auto &p : b->events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    b->events.clear();
+    b->profiling = enable != 0;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_profile_read(icar_adv_batch_t *b, double *step_ms, int64_t *steps, int64_t *kernels_per_step,
+                                int64_t *cell_species_per_step)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    cudaSetDevice(b->device);
+    BCUDA(b, cudaStreamSynchronize(b->stream));
+    double ms = 0.0;
+    for (auto &p : b->events) {
+        float t = 0.0f;
+        BCUDA(b, cudaEventElapsedTime(&t, p.first, p.second));
+        ms += t;
+    }
+    if (step_ms) *step_ms = ms;
+    if (steps) *steps = (int64_t)b->events.size();
+    if (kernels_per_step)
+        *kernels_per_step = (b->n_force > 0) + (b->n_prep > 0) + (b->n_up > 0) + (b->n_items > 0);
+    if (cell_species_per_step) {
+        int64_t cs = 0;
+        for (icar_adv_t *h : b->members) cs += (int64_t)h->g.nx * h->g.ny * h->g.nz * h->desc.n_species;
+        *cell_species_per_step = cs;
+    }
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_destroy(icar_adv_batch_t *b)
+{
+    if (!b) return ICAR_ADV_OK;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    for (icar_adv_t *h : b->members) {
+        h->batch = nullptr;
+        h->stream = h->own_stream;
+    }
+    drop_graphs(b);
+    for (auto &p : b->events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    if (b->d_mem[0]) cudaFree(b->d_mem[0]);
+    if (b->d_mem[1]) cudaFree(b->d_mem[1]);
+    if (b->d_ints) cudaFree(b->d_ints);
+    if (b->d_pairs) cudaFree(b->d_pairs);
+    if (b->d_items) cudaFree(b->d_items);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return ICAR_ADV_OK;
+}
+
+const char *icar_adv_batch_last_error(const icar_adv_batch_t *b) { return b ? b->err.c_str() : g_create_error.c_str(); }
 
 }  // extern "C"

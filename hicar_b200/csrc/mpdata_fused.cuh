@@ -132,13 +132,19 @@ __global__ void k_mp_upwind(Geo g, SpeciesPtrs sp, const float *__restrict__ U, 
 
 namespace mpf {
 constexpr int TX = 28;            // output columns per tile
-constexpr int TY = 16;            // output rows per tile
 constexpr int PW = 32;            // plane width: x from i0-2 to i0+29
-constexpr int PH = TY + 4;        // plane height: y from j0-2 to j0+TY+1
-constexpr int PLANE = PW * PH;
-constexpr int NT = 256;
-constexpr int NW = NT / 32;
-constexpr int RPW = TY / NW;      // output rows per warp
+// Tile heights: TY output rows, NW warps, TY/NW output rows per warp; the
+// plane holds TY+4 rows (y from j0-2 to j0+TY+1).
+template <int TY_, int NW_>
+struct Shape {
+    static constexpr int TY = TY_;
+    static constexpr int NW = NW_;
+    static constexpr int NT = 32 * NW_;
+    static constexpr int PH = TY_ + 4;
+    static constexpr int PLANE = PW * PH;
+    static constexpr int RPW = TY_ / NW_;
+    static_assert(TY_ % NW_ == 0, "rows per warp must be whole");
+};
 // shared-memory plane slots
 constexpr int S_Q1 = 0;           // 4 ring slots: level l -> S_Q1 + (l & 3)
 constexpr int S_Q0 = 4;           // 3 ring slots: level l -> S_Q0 + l % 3
@@ -151,7 +157,8 @@ constexpr int S_BXI = 21, S_BXO = 22, S_BYI = 23, S_BYO = 24;
 constexpr int S_U2L = 25;         // 2 ring slots
 constexpr int S_V2L = 27;         // 2 ring slots
 constexpr int NPLANES = 29;
-constexpr size_t SMEM = (size_t)NPLANES * PLANE * sizeof(float);
+template <class SH>
+constexpr size_t smem_bytes() { return (size_t)NPLANES * SH::PLANE * sizeof(float); }
 }  // namespace mpf
 
 __device__ __forceinline__ void cp_async16(float *dst, const float *src, bool valid)
@@ -180,10 +187,11 @@ __device__ __forceinline__ float fct_beta(float num, float den)
 // chunk is either wholly inside a row's pitch (valid cells, or the zero
 // padding past nx) or wholly outside the field and zero-filled.  ey is the
 // y extent of the field (ny, or ny+1 for y-face fields).
+template <class SH>
 __device__ __forceinline__ void load_plane(float *dst, const float *__restrict__ src, const Geo &g, int lev, int i0,
                                            int j0, int ey)
 {
-    for (int e = threadIdx.x; e < (mpf::PW / 4) * mpf::PH; e += mpf::NT) {
+    for (int e = threadIdx.x; e < (mpf::PW / 4) * SH::PH; e += SH::NT) {
         const int cx = e % (mpf::PW / 4), ly = e / (mpf::PW / 4);
         const int i = i0 - 2 + 4 * cx, j = j0 - 2 + ly;
         const bool ok = i >= 0 && i < g.P && j >= 0 && j < ey;
@@ -191,48 +199,41 @@ __device__ __forceinline__ void load_plane(float *dst, const float *__restrict__
     }
 }
 
-// q/d for the limiter-free divisions of the pseudo-velocity and corrective
-// passes; a zero numerator over a positive denominator is returned as is
-// (the exact IEEE quotient), which skips the division in empty regions.
-__device__ __forceinline__ float div0(float n, float d)
-{
-    if (n == 0.0f && d > 0.0f) return n;
-    return n / d;
-}
+// IEEE-rounded quotient (a zero-numerator shortcut was measured slower: the
+// branch costs more than the divisions it skips in mixed warps).
+__device__ __forceinline__ float div0(float n, float d) { return n / d; }
 
-template <bool FCT>
-__global__ void __launch_bounds__(mpf::NT, 3)
-    k_mp_corr(Geo g, SpeciesPtrs sp, int nspecies, int tiles_x, const float *__restrict__ Um,
-              const float *__restrict__ Vm, const float *__restrict__ Wp, const float *__restrict__ Gc,
-              const float *__restrict__ DJR, const float *__restrict__ dz)
+// One 28 x TY column tile of one species: the z-march described at the top
+// of this file.  i0 is the first output column (i0-2 a multiple of 4), j0
+// the first output row; sm is the CTA's dynamic shared memory.
+template <bool FCT, class SH>
+__device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const float *__restrict__ q0g,
+                                             const float *__restrict__ q1g, float *__restrict__ outg, int i0, int j0,
+                                             const float *__restrict__ Um, const float *__restrict__ Vm,
+                                             const float *__restrict__ Wp, const float *__restrict__ Gc,
+                                             const float *__restrict__ DJR, const float *__restrict__ dz)
 {
     using namespace mpf;
-    extern __shared__ float sm[];
-    const int s = blockIdx.x % nspecies;
-    const int tile = blockIdx.x / nspecies;
-    const int i0 = (tile % tiles_x) * TX - 2;  // first output column; i0-2 is a multiple of 4
-    const int j0 = 1 + (tile / tiles_x) * TY;
+    constexpr int TY = SH::TY, NW = SH::NW, PH = SH::PH, PLANE = SH::PLANE, RPW = SH::RPW;
+    (void)PH;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const float *__restrict__ q0g = sp.q0[s];
-    const float *__restrict__ q1g = sp.q1[s];
-    float *__restrict__ outg = sp.out[s];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const float e10 = 1e-10f, e15 = 1e-15f, q4 = 1.0f / 4.0f;
     auto P = [&](int slot) { return sm + (size_t)slot * PLANE; };
 #define AT(slot, lx, ly) sm[(size_t)(slot) * PLANE + (ly) * PW + (lx)]
 
     // ---- prologue: levels 0 and 1 of everything the first iteration reads
-    load_plane(P(S_Q1 + 0), q1g, g, 0, i0, j0, ny);
-    load_plane(P(S_Q0 + 0), q0g, g, 0, i0, j0, ny);
-    load_plane(P(S_U + 0), Um, g, 0, i0, j0, ny);
-    load_plane(P(S_V + 0), Vm, g, 0, i0, j0, ny + 1);
-    load_plane(P(S_W + 0), Wp, g, 0, i0, j0, ny);
-    load_plane(P(S_G + 0), Gc, g, 0, i0, j0, ny);
-    load_plane(P(S_Q1 + 1), q1g, g, 1, i0, j0, ny);
-    load_plane(P(S_Q0 + 1), q0g, g, 1, i0, j0, ny);
-    load_plane(P(S_U + 1), Um, g, 1, i0, j0, ny);
-    load_plane(P(S_V + 1), Vm, g, 1, i0, j0, ny + 1);
-    load_plane(P(S_G + 1), Gc, g, 1, i0, j0, ny);
+    load_plane<SH>(P(S_Q1 + 0), q1g, g, 0, i0, j0, ny);
+    load_plane<SH>(P(S_Q0 + 0), q0g, g, 0, i0, j0, ny);
+    load_plane<SH>(P(S_U + 0), Um, g, 0, i0, j0, ny);
+    load_plane<SH>(P(S_V + 0), Vm, g, 0, i0, j0, ny + 1);
+    load_plane<SH>(P(S_W + 0), Wp, g, 0, i0, j0, ny);
+    load_plane<SH>(P(S_G + 0), Gc, g, 0, i0, j0, ny);
+    load_plane<SH>(P(S_Q1 + 1), q1g, g, 1, i0, j0, ny);
+    load_plane<SH>(P(S_Q0 + 1), q0g, g, 1, i0, j0, ny);
+    load_plane<SH>(P(S_U + 1), Um, g, 1, i0, j0, ny);
+    load_plane<SH>(P(S_V + 1), Vm, g, 1, i0, j0, ny + 1);
+    load_plane<SH>(P(S_G + 1), Gc, g, 1, i0, j0, ny);
     cp_async_commit();
 
     // per-output-cell z state (two output rows per warp)
@@ -252,13 +253,13 @@ __global__ void __launch_bounds__(mpf::NT, 3)
         __syncthreads();
         // prefetch the levels the next iteration adds: q1/q0/U/V/G at t+2, W' at t+1
         if (t + 2 < nz) {
-            load_plane(P(S_Q1 + ((t + 2) & 3)), q1g, g, t + 2, i0, j0, ny);
-            load_plane(P(S_Q0 + (t + 2) % 3), q0g, g, t + 2, i0, j0, ny);
-            load_plane(P(S_U + (t + 2) % 3), Um, g, t + 2, i0, j0, ny);
-            load_plane(P(S_V + (t + 2) % 3), Vm, g, t + 2, i0, j0, ny + 1);
-            load_plane(P(S_G + (t + 2) % 3), Gc, g, t + 2, i0, j0, ny);
+            load_plane<SH>(P(S_Q1 + ((t + 2) & 3)), q1g, g, t + 2, i0, j0, ny);
+            load_plane<SH>(P(S_Q0 + (t + 2) % 3), q0g, g, t + 2, i0, j0, ny);
+            load_plane<SH>(P(S_U + (t + 2) % 3), Um, g, t + 2, i0, j0, ny);
+            load_plane<SH>(P(S_V + (t + 2) % 3), Vm, g, t + 2, i0, j0, ny + 1);
+            load_plane<SH>(P(S_G + (t + 2) % 3), Gc, g, t + 2, i0, j0, ny);
         }
-        if (t + 1 < nz) load_plane(P(S_W + (t + 1) % 3), Wp, g, t + 1, i0, j0, ny);
+        if (t + 1 < nz) load_plane<SH>(P(S_W + (t + 1) % 3), Wp, g, t + 1, i0, j0, ny);
         cp_async_commit();
 
         const bool haveA = t < nz;
@@ -567,14 +568,30 @@ __global__ void __launch_bounds__(mpf::NT, 3)
             }
         }
     }
+    __syncthreads();  // the CTA may start another tile in the same shared memory
 #undef AT
+}
+
+template <bool FCT, class SH>
+__global__ void __launch_bounds__(SH::NT, (SH::NT <= 128 ? 5 : 3))
+    k_mp_corr(Geo g, SpeciesPtrs sp, int nspecies, int tiles_x, const float *__restrict__ Um,
+              const float *__restrict__ Vm, const float *__restrict__ Wp, const float *__restrict__ Gc,
+              const float *__restrict__ DJR, const float *__restrict__ dz)
+{
+    extern __shared__ float4 sm4[];
+    const int s = blockIdx.x % nspecies;
+    const int tile = blockIdx.x / nspecies;
+    const int i0 = (tile % tiles_x) * mpf::TX - 2;  // first output column; i0-2 is a multiple of 4
+    const int j0 = 1 + (tile / tiles_x) * SH::TY;
+    mp_corr_tile<FCT, SH>(reinterpret_cast<float *>(sm4), g, sp.q0[s], sp.q1[s], sp.out[s], i0, j0, Um, Vm, Wp, Gc,
+                          DJR, dz);
 }
 
 inline bool fused_eligible(int order, int fct) { return order == 2 && (fct == 0 || fct == 1); }
 
 // tile tx covers output columns [TX*tx-2, TX*tx+TX-2); the last must reach nx-2
 inline int mp_tiles_x(const Geo &g) { return g.nx / mpf::TX + 1; }
-inline int mp_tiles_y(const Geo &g) { return (g.ny - 2 + mpf::TY - 1) / mpf::TY; }
+inline int mp_tiles_y(const Geo &g, int ty) { return (g.ny - 2 + ty - 1) / ty; }
 
 // Debug check (parameters%debug): flags any interior cell whose donor-cell
 // outflow fraction, sum of outgoing Courant fluxes over J*rho (dz*J*rho for
@@ -611,6 +628,68 @@ inline int check_courant(cudaStream_t st, const Geo &g, const float *Um, const f
     cudaFreeAsync(flag, st);
     cudaStreamSynchronize(st);
     return host;
+}
+
+}  // namespace icar
+
+namespace icar {
+
+// Tile shapes of the fused correction kernel (selected per grid shape by
+// the autotuner): output rows per tile and warps per CTA.
+using MpShape8 = mpf::Shape<8, 4>;
+using MpShape16 = mpf::Shape<16, 8>;
+using MpShape24 = mpf::Shape<24, 8>;
+using MpShape32 = mpf::Shape<32, 8>;
+constexpr int MP_NSHAPES = 4;
+inline int mp_shape_ty(int shape)
+{
+    const int ty[MP_NSHAPES] = {8, 16, 24, 32};
+    return ty[shape < 0 || shape >= MP_NSHAPES ? 1 : shape];
+}
+
+template <class SH>
+inline cudaError_t mp_corr_attr()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_mp_corr<true, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)mpf::smem_bytes<SH>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mp_corr<false, SH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)mpf::smem_bytes<SH>());
+    return e;
+}
+
+// Allow every instantiation its dynamic shared memory (once per device).
+inline cudaError_t mp_corr_setup()
+{
+    cudaError_t e = mp_corr_attr<MpShape8>();
+    if (e == cudaSuccess) e = mp_corr_attr<MpShape16>();
+    if (e == cudaSuccess) e = mp_corr_attr<MpShape24>();
+    if (e == cudaSuccess) e = mp_corr_attr<MpShape32>();
+    return e;
+}
+
+template <class SH>
+inline void mp_corr_launch_t(cudaStream_t st, const Geo &g, const SpeciesPtrs &sp, int S, int fct, const float *Um,
+                             const float *Vm, const float *Wp, const float *Gc, const float *DJR, const float *dz)
+{
+    const int tx = mp_tiles_x(g), ty = mp_tiles_y(g, SH::TY);
+    const unsigned nblk = (unsigned)(tx * ty * S);
+    if (fct)
+        k_mp_corr<true, SH><<<nblk, SH::NT, mpf::smem_bytes<SH>(), st>>>(g, sp, S, tx, Um, Vm, Wp, Gc, DJR, dz);
+    else
+        k_mp_corr<false, SH><<<nblk, SH::NT, mpf::smem_bytes<SH>(), st>>>(g, sp, S, tx, Um, Vm, Wp, Gc, DJR, dz);
+}
+
+inline void mp_corr_launch(cudaStream_t st, int shape, const Geo &g, const SpeciesPtrs &sp, int S, int fct,
+                           const float *Um, const float *Vm, const float *Wp, const float *Gc, const float *DJR,
+                           const float *dz)
+{
+    switch (shape) {
+    case 0: mp_corr_launch_t<MpShape8>(st, g, sp, S, fct, Um, Vm, Wp, Gc, DJR, dz); break;
+    case 2: mp_corr_launch_t<MpShape24>(st, g, sp, S, fct, Um, Vm, Wp, Gc, DJR, dz); break;
+    case 3: mp_corr_launch_t<MpShape32>(st, g, sp, S, fct, Um, Vm, Wp, Gc, DJR, dz); break;
+    default: mp_corr_launch_t<MpShape16>(st, g, sp, S, fct, Um, Vm, Wp, Gc, DJR, dz); break;
+    }
 }
 
 }  // namespace icar

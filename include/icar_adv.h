@@ -200,6 +200,40 @@ int icar_adv_profile(icar_adv_t *h, int32_t enable);
 int icar_adv_profile_read(icar_adv_t *h, double *species_kernel_ms, int64_t *species_kernel_launches,
                           int64_t *all_launches, int64_t *species_passes);
 
+/* ---------------------------------------------------------------------------
+ * Batched form (no reference counterpart: the reference advances one domain
+ * per process).  Many independent domains -- ensemble members or served
+ * requests of uneven nx x ny x nz -- advance together: one step is a single
+ * CUDA-graph launch holding the boundary update, the per-step wind fields,
+ * the donor-cell pass and one persistent correction kernel over a
+ * (member, species, tile) work list.  Each member keeps its own device
+ * fields; while it is a member its work runs on the batch's stream, it
+ * cannot be stepped on its own, and set/get_field stay available.  All
+ * members must use MPDATA order 2 without RK3 and share MPDATA_FCT.
+ * A step applies apply_forcing(dt) then advect(real(dt)) to every member,
+ * with each member's own dt (icar_adv_step without enforce_limits).
+ * ------------------------------------------------------------------------- */
+int icar_adv_batch_create(int32_t device, icar_adv_batch_t **out);
+int icar_adv_batch_destroy(icar_adv_batch_t *b);
+int icar_adv_batch_add(icar_adv_batch_t *b, icar_adv_t *member, double dt_seconds);
+int icar_adv_batch_remove(icar_adv_batch_t *b, icar_adv_t *member);
+int icar_adv_batch_set_dt(icar_adv_batch_t *b, icar_adv_t *member, double dt_seconds);
+int icar_adv_batch_set_tile_shape(icar_adv_batch_t *b, int32_t shape);
+int icar_adv_batch_step(icar_adv_batch_t *b);
+int icar_adv_batch_sync(icar_adv_batch_t *b);
+int icar_adv_batch_set_stream(icar_adv_batch_t *b, void *cuda_stream);
+/* Event timing of every step launched while enabled; reading synchronises. */
+int icar_adv_batch_profile(icar_adv_batch_t *b, int32_t enable);
+int icar_adv_batch_profile_read(icar_adv_batch_t *b, double *step_ms, int64_t *steps, int64_t *kernels_per_step,
+                                int64_t *cell_species_per_step);
+const char *icar_adv_batch_last_error(const icar_adv_batch_t *b);
+
+/* Tile shape of the fused MPDATA kernel (no reference counterpart; chosen per
+ * grid shape by the autotuner).  icar_adv_tile_shapes reports how many shapes
+ * exist and the output rows per tile of each (rows may be NULL). */
+int icar_adv_set_tile_shape(icar_adv_t *h, int32_t shape);
+int icar_adv_tile_shapes(int32_t *n_shapes, int32_t *rows);
+
 /* Kernel selection for testing: 0 = fused MPDATA kernel where it applies
  * (default), 1 = the staged one-stage-per-kernel path. */
 int icar_adv_set_path(icar_adv_t *h, int32_t path);
