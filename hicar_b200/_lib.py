@@ -57,6 +57,20 @@ class Opts(C.Structure):
     ]
 
 
+class NoallocArgs(C.Structure):
+    """icar_adv_noalloc_args: device pointers in the pitched layout."""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("dx", C.c_float), ("dt", C.c_float),
+        ("mpdata_fct", C.c_int32), ("advect_density", C.c_int32), ("n_species", C.c_int32),
+        ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p), ("density", C.c_void_p),
+        ("jacobian", C.c_void_p), ("jacobian_u", C.c_void_p), ("jacobian_v", C.c_void_p),
+        ("jacobian_w", C.c_void_p), ("advection_dz", C.c_void_p),
+        ("q_in", C.c_void_p * MAX_SPECIES), ("q_out", C.c_void_p * MAX_SPECIES),
+        ("stream", C.c_void_p),
+    ]
+
+
 # every exported entry point, with argument and result types
 _PROTOS = {
     "icar_adv_abi_version": (C.c_int, []),
@@ -95,6 +109,7 @@ _PROTOS = {
     "icar_adv_batch_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                               C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "icar_adv_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "icar_adv_advect_noalloc": (C.c_int, [C.POINTER(NoallocArgs)]),
     "icar_adv_tile_shapes": (C.c_int, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "icar_adv_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                         C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

@@ -1424,3 +1424,109 @@ int icar_adv_batch_destroy(icar_adv_batch_t *b)
 const char *icar_adv_batch_last_error(const icar_adv_batch_t *b) { return b ? b->err.c_str() : g_create_error.c_str(); }
 
 }  // extern "C"
+
+// ===========================================================================
+// MPDATA step into caller-owned device memory, allocating nothing
+// ===========================================================================
+// For callers that cannot allocate device memory themselves (see
+// icar_adv_advect_noalloc in include/icar_adv.h).  The per-step scratch of
+// the fused path (U_m, V_m, W_m, J*rho, dz*J*rho, W_m/dz and one pass-1
+// field) lives in this file-scope array instead of cudaMalloc'ed buffers.
+// Every GPU that loads the library holds it until the process exits, and
+// every call on a device shares it.
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_FLOATS = (size_t)4 << 20;  // 4 Mi floats = 16 MiB per device
+__device__ __align__(256) float g_noalloc_scratch[NOALLOC_SCRATCH_FLOATS];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+float *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};  // device address of g_noalloc_scratch, per device
+
+// Once per device, with that device current: the array's device address (a
+// host-side `g_noalloc_scratch` is only a stand-in symbol, not a pointer the
+// kernels may use) and the fused kernel's shared-memory opt-in.
+int noalloc_setup(int dev, float **out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        float *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(nullptr, ICAR_ADV_CUDA_ERROR, "cudaGetSymbolAddress of the static scratch failed: %s",
+                        cudaGetErrorString(e));
+        e = icar::mp_corr_setup();
+        if (e != cudaSuccess)
+            return fail(nullptr, ICAR_ADV_CUDA_ERROR, "kernel setup failed: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return ICAR_ADV_OK;
+}
+
+inline size_t round64(size_t n) { return (n + 63) / 64 * 64; }
+
+}  // namespace
+
+extern "C" int icar_adv_advect_noalloc(const icar_adv_noalloc_args *a)
+{
+    if (!a) return fail(nullptr, ICAR_ADV_BAD_ARG, "args is NULL");
+    if (a->nx < 3 || a->ny < 3 || a->nz < 3)
+        return fail(nullptr, ICAR_ADV_BAD_ARG, "domain %dx%dx%d too small (each extent must be >= 3)", a->nx, a->ny,
+                    a->nz);
+    if (a->n_species < 0 || a->n_species > ICAR_ADV_MAX_SPECIES)
+        return fail(nullptr, ICAR_ADV_BAD_ARG, "n_species %d out of range", a->n_species);
+    if (!(a->dx > 0.0f) || !std::isfinite(a->dx) || !(a->dt >= 0.0f) || !std::isfinite(a->dt))
+        return fail(nullptr, ICAR_ADV_BAD_ARG, "dx must be positive and dt finite and >= 0");
+    if (!a->u || !a->v || !a->w || !a->density || !a->jacobian || !a->jacobian_u || !a->jacobian_v ||
+        !a->jacobian_w || !a->advection_dz)
+        return fail(nullptr, ICAR_ADV_BAD_ARG, "a wind or metric field pointer is NULL");
+    for (int s = 0; s < a->n_species; s++) {
+        if (!a->q_in[s] || !a->q_out[s]) return fail(nullptr, ICAR_ADV_BAD_ARG, "species %d pointer is NULL", s);
+        if (a->q_in[s] == a->q_out[s])
+            return fail(nullptr, ICAR_ADV_BAD_ARG, "species %d: q_out must not alias q_in", s);
+    }
+    Geo g;
+    g.nx = a->nx;
+    g.ny = a->ny;
+    g.nz = a->nz;
+    g.P = ((a->nx + 1) + 3) / 4 * 4;
+    const size_t nc = (size_t)g.P * g.nz * g.ny, nv = (size_t)g.P * g.nz * (g.ny + 1);
+    // U_m (nc), V_m (nv), then W_m, G, DJR, W', q1 (nc each), each 256-byte aligned
+    const size_t need = round64(nc) * 6 + round64(nv);
+    if (need > NOALLOC_SCRATCH_FLOATS)
+        return fail(nullptr, ICAR_ADV_BAD_ARG,
+                    "domain %dx%dx%d needs %zu floats of scratch; the static scratch holds %zu "
+                    "(use the handle API, which allocates, for larger domains)",
+                    a->nx, a->ny, a->nz, need, NOALLOC_SCRATCH_FLOATS);
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fail(nullptr, ICAR_ADV_CUDA_ERROR, "no usable current device: %s", cudaGetErrorString(ce));
+    float *base = nullptr;
+    int e = noalloc_setup(dev, &base);
+    if (e) return e;
+    cudaStream_t st = (cudaStream_t)a->stream;
+    float *Um = base, *Vm = Um + round64(nc), *Wm = Vm + round64(nv), *Gc = Wm + round64(nc),
+          *DJR = Gc + round64(nc), *Wp = DJR + round64(nc), *q1 = Wp + round64(nc);
+    // the array keeps the previous call's contents; the padding columns the
+    // tile loads read must start at zero, so clear the part this call uses
+    ce = cudaMemsetAsync(base, 0, need * sizeof(float), st);
+    if (ce != cudaSuccess) return fail(nullptr, ICAR_ADV_CUDA_ERROR, "cudaMemsetAsync: %s", cudaGetErrorString(ce));
+    const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+    icar::k_mp_prep<<<blocks_for(nf, 256), 256, 0, st>>>(g, a->dx, a->dt, a->advect_density, a->u, a->v, a->w,
+                                                       a->density, a->jacobian, a->jacobian_u, a->jacobian_v,
+                                                       a->jacobian_w, a->advection_dz, Um, Vm, Wm, Gc, DJR, Wp);
+    const size_t ncell = (size_t)g.nx * g.nz * g.ny;
+    for (int s = 0; s < a->n_species; s++) {
+        icar::SpeciesPtrs sp{};
+        sp.q0[0] = a->q_in[s];
+        sp.q1[0] = q1;
+        sp.out[0] = a->q_out[s];
+        icar::k_mp_upwind<<<dim3(blocks_for(ncell, 256), 1), 256, 0, st>>>(g, sp, Um, Vm, Wm, Gc, DJR);
+        icar::mp_corr_launch(st, 1, g, sp, 1, a->mpdata_fct ? 1 : 0, Um, Vm, Wp, Gc, DJR, a->advection_dz);
+    }
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) return fail(nullptr, ICAR_ADV_CUDA_ERROR, "launch failed: %s", cudaGetErrorString(ce));
+    return ICAR_ADV_OK;
+}

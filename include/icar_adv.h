@@ -228,6 +228,55 @@ int icar_adv_batch_profile_read(icar_adv_batch_t *b, double *step_ms, int64_t *s
                                 int64_t *cell_species_per_step);
 const char *icar_adv_batch_last_error(const icar_adv_batch_t *b);
 
+/* ---------------------------------------------------------------------------
+ * MPDATA step on caller-owned device arrays that allocates nothing.  This
+ * entry point has no counterpart in the reference.  It is for callers that
+ * cannot call cudaMalloc: code running inside another framework's memory
+ * pool or allocator (which must own every device allocation), inside a
+ * captured CUDA graph or a stream-ordered region where an allocation would
+ * synchronise or break the capture, or under a fixed device-memory budget.
+ * The caller passes the inputs and outputs; the library's per-step scratch
+ * (Courant fluxes, J*rho, dz*J*rho, W_m/dz and one pass-1 field) comes from a
+ * file-scope __device__ array of 4 Mi floats (16 MiB) that every GPU that
+ * loads the library holds until the process exits.
+ *
+ * Limit: the domain must fit that array: 6*round64(P*nz*ny) +
+ * round64(P*nz*(ny+1)) <= 4*2^20 floats, with P = round_up(nx+1, 4) and
+ * round64 rounding up to a multiple of 64 (about 600 thousand cells, e.g.
+ * 128x128x32); larger domains get ICAR_ADV_BAD_ARG with the sizes in the
+ * message.  The scheme is advect() with MPDATA order 2 (FCT on or off):
+ * every species is read from q_in[s] and the new state written to q_out[s]
+ * (no aliasing); no boundary update.
+ *
+ * Device layout of every array: the reference's Fortran order with row pitch
+ * P floats, element (i,k,j) at i + P*(k + nz*j); x-face fields (u,
+ * jacobian_u) use i <= nx, y-face fields (v, jacobian_v) have ny+1 rows, cell
+ * fields i < nx.  Padding columns are ignored on input and left untouched
+ * on output.
+ *
+ * The first call on a device sets that device up (it looks up the device
+ * address of the static array and opts the kernel into its shared memory):
+ * make it before any stream capture.  Every call on a device shares the one
+ * array, and each call clears the part it uses at its start, so calls whose
+ * work overlaps on the GPU (other streams, other host threads) race: order
+ * them on one stream or synchronise between them.  Work is enqueued on
+ * `stream` (NULL = the legacy default stream); the call returns without
+ * waiting. */
+typedef struct {
+    int32_t nx, ny, nz;
+    float dx;                 /* domain%dx in metres       */
+    float dt;                 /* seconds                   */
+    int32_t mpdata_fct;       /* MPDATA_FCT                */
+    int32_t advect_density;   /* parameters%advect_density */
+    int32_t n_species;
+    const float *u, *v, *w, *density, *jacobian, *jacobian_u, *jacobian_v, *jacobian_w, *advection_dz;
+    const float *q_in[ICAR_ADV_MAX_SPECIES];
+    float *q_out[ICAR_ADV_MAX_SPECIES];
+    void *stream;             /* cudaStream_t */
+} icar_adv_noalloc_args;
+
+int icar_adv_advect_noalloc(const icar_adv_noalloc_args *args);
+
 /* Tile shape of the fused MPDATA kernel (no reference counterpart; chosen per
  * grid shape by the autotuner).  icar_adv_tile_shapes reports how many shapes
  * exist and the output rows per tile of each (rows may be NULL). */
