@@ -44,7 +44,10 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="full_species",
-                   choices=["full_species", "plain_c1", "mid_species", "ensemble"])
+                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served"])
+    p.add_argument("--serve-rate", type=float, default=20.0)
+    p.add_argument("--serve-duration", type=float, default=6.0)
+    p.add_argument("--serve-steps-scale", type=float, default=0.1)
     p.add_argument("--members", type=int, default=64, help="ensemble size (ensemble workload)")
     p.add_argument("--tile-shape", type=int, default=1, help="fused-kernel tile shape 0..3 (8/16/24/32 rows)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -506,12 +509,48 @@ def run_ensemble(args):
         dist.destroy_process_group()
 
 
+# -------------------------------------------------------------- served
+def run_served(args):
+    """Poisson arrivals of downscaling requests into the continuous-batching
+    server (config 4's size distributions; the arrival window and the step
+    counts are scaled by --serve-duration and --serve-steps-scale so a run
+    fits in minutes)."""
+    import torch
+    from hicar_b200.serve import Server, poisson_requests
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    smin, smax = int(round(50 * args.serve_steps_scale)), int(round(500 * args.serve_steps_scale))
+    reqs = poisson_requests(args.serve_rate, args.serve_duration, seed=11, steps=(max(1, smin), max(1, smax)))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    srv = Server(device=local, budget_bytes=150e9, keep_results=False, stream=stream.cuda_stream)
+    for r in reqs:
+        srv.submit(r)
+    clocks = ClockSampler(local)
+    clocks.start()
+    srv.t0 = time.perf_counter()
+    srv.run()
+    clk = clocks.stop()
+    rep = srv.report()
+    srv.close()
+    print(json.dumps({
+        "metric": METRIC + " (served)", "value": rep.get("throughput_cell_species_per_s"), "unit": UNIT,
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"served requests: Poisson {args.serve_rate} req/s for {args.serve_duration} s, "
+                               f"area lognormal median 256^2 (sides 64..1024), nz U[20,60], 12 fields, "
+                               f"steps U[{smin},{smax}], HBM admission budget 150 GB"},
+        "serving": rep, "clocks": clk}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble(args)
+    elif args.workload == "served":
+        run_served(args)
     else:
         run_b200(args)
 

@@ -109,6 +109,55 @@ class Domain:
         d.adv_vars = {k: np.ascontiguousarray(v, np.float32).copy() for k, v in case.species.items()}
         return d
 
+    @classmethod
+    def create_on_device(cls, fields: dict, nx: int, ny: int, nz: int, dx: float, options: "Options",
+                         device: int = 0, forcing: bool = False) -> "Domain":
+        """adv_init from CUDA tensors already in device memory (Fortran layout,
+        contiguous): fields holds the nine wind/metric fields and
+        fields["species"] the advected ones.  forcing=True fixes every
+        species' boundary forcing at its initial value."""
+        import torch
+        torch.cuda.current_stream(device).synchronize()   # the tensors must be complete before the copies
+        d = cls(nx, ny, nz, dx, device=device)
+        d._device_fields = fields
+        names = list(fields["species"])
+        d.adv_vars = {k: None for k in names}
+        lib = L.load()
+        desc = d._desc(names)
+        opts = options.to_c()
+        h = C.c_void_p()
+        L.check(lib.icar_adv_create(C.byref(desc), C.byref(opts), C.byref(h)))
+        d._h = h
+        d._options = options
+        for k, fid in _METRIC_FIELDS.items():
+            L.check(lib.icar_adv_set_field_device(h, fid, C.c_void_p(fields[k].data_ptr())), h)
+        for k in names:
+            t = fields["species"][k]
+            L.check(lib.icar_adv_set_field_device(h, L.SPECIES_IDS[k], C.c_void_p(t.data_ptr())), h)
+            if forcing:
+                L.check(lib.icar_adv_set_field_device(h, L.F_FORCING_BASE + L.SPECIES_IDS[k],
+                                                      C.c_void_p(t.data_ptr())), h)
+        L.check(lib.icar_adv_sync(h), h)
+        return d
+
+    def fetch_device(self, name: str, out) -> None:
+        """Copy a resident species into a contiguous CUDA tensor (Fortran layout)."""
+        L.check(L.load().icar_adv_get_field_device(self.handle, self._field_id(name), C.c_void_p(out.data_ptr())),
+                self.handle)
+
+    def _desc(self, names) -> "L.Desc":
+        desc = L.Desc()
+        desc.nx, desc.ny, desc.nz, desc.dx = self.nx, self.ny, self.nz, self.dx
+        if len(names) > L.MAX_SPECIES:
+            raise ValueError("too many advected species")
+        desc.n_species = len(names)
+        for i, n in enumerate(names):
+            desc.species[i] = L.SPECIES_IDS[n]
+        desc.north_boundary, desc.south_boundary = int(self.north_boundary), int(self.south_boundary)
+        desc.east_boundary, desc.west_boundary = int(self.east_boundary), int(self.west_boundary)
+        desc.device = self.device
+        return desc
+
     # -- handle plumbing -------------------------------------------------
     @property
     def handle(self):
@@ -229,17 +278,8 @@ def adv_init(domain: Domain, options: Options) -> None:
     lib = L.load()
     if domain._h is not None:
         domain.close()
-    desc = L.Desc()
-    desc.nx, desc.ny, desc.nz, desc.dx = domain.nx, domain.ny, domain.nz, domain.dx
     names = list(domain.adv_vars)
-    if len(names) > L.MAX_SPECIES:
-        raise ValueError("too many advected species")
-    desc.n_species = len(names)
-    for i, n in enumerate(names):
-        desc.species[i] = L.SPECIES_IDS[n]
-    desc.north_boundary, desc.south_boundary = int(domain.north_boundary), int(domain.south_boundary)
-    desc.east_boundary, desc.west_boundary = int(domain.east_boundary), int(domain.west_boundary)
-    desc.device = domain.device
+    desc = domain._desc(names)
     opts = options.to_c()
     h = C.c_void_p()
     L.check(lib.icar_adv_create(C.byref(desc), C.byref(opts), C.byref(h)))

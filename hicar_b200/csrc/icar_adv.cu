@@ -169,7 +169,9 @@ int64_t footprint_bytes(const icar_adv_desc &d, const icar_adv_opts &o)
     total += f * (int64_t)(nu + nv + nc + nc * 2 + nu + nv + nc * 2);  // u v w rho jac ju jv jw dz
     total += f * (int64_t)nc * (d.n_species + 1);                      // species + spare
     total += f * (int64_t)(nu + nv + nc);                              // Um Vm Wm
-    if (o.advection == ICAR_ADV_MPDATA)
+    if (o.advection == ICAR_ADV_MPDATA && !o.rk3 && icar::fused_eligible(o.mpdata_order, o.mpdata_fct))
+        total += f * (int64_t)nc * (2 * d.n_species + 3);              // fused: next + pass-1 per species, G, DJR, W'
+    else if (o.advection == ICAR_ADV_MPDATA)
         total += f * (int64_t)(nc + 2 * (nu + nv + nc));               // staged scratch
     else
         total += f * (int64_t)(2 * (nu + nv + nzf) + 4 * nc);
@@ -457,6 +459,14 @@ int compute_wind(icar_adv_t *h, float dt)
 int mpdata_staged(icar_adv_t *h, int s)
 {
     const Geo &g = h->g;
+    {
+        const size_t nc = h->n_cell, nu = h->n_u, nv = h->n_v;
+        int e;
+        if ((e = alloc(h, h->q1, nc)) || (e = alloc(h, h->u2, nu)) || (e = alloc(h, h->v2, nv)) ||
+            (e = alloc(h, h->w2, nc)) || (e = alloc(h, h->u2l, nu)) || (e = alloc(h, h->v2l, nv)) ||
+            (e = alloc(h, h->w2l, nc)))
+            return e;
+    }
     float *q = h->q[s].p;
     const size_t nc = (size_t)g.nx * g.nz * g.ny;
     const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
@@ -741,10 +751,7 @@ int icar_adv_create(const icar_adv_desc *desc, const icar_adv_opts *opts, icar_a
     for (int s = 0; s < S; s++)
         if ((e = alloc(h, h->q[s], nc))) return bail(e);
     if (opts->advection == ICAR_ADV_MPDATA) {
-        if ((e = alloc(h, h->q1, nc)) || (e = alloc(h, h->u2, nu)) || (e = alloc(h, h->v2, nv)) ||
-            (e = alloc(h, h->w2, nc)) || (e = alloc(h, h->u2l, nu)) || (e = alloc(h, h->v2l, nv)) ||
-            (e = alloc(h, h->w2l, nc)))
-            return bail(e);
+        // the staged MPDATA scratch is allocated on first use (mpdata_staged)
     } else {
         if ((e = alloc(h, h->fx, nu)) || (e = alloc(h, h->fy, nv)) || (e = alloc(h, h->fz, h->n_zf)) ||
             (e = alloc(h, h->temp, nc)))

@@ -304,3 +304,81 @@ def periodic_y_case(ny: int = 100, nx: int = 3, nz: int = 3, cfl: float = 0.25, 
                 jacobian_w=np.ones((ny, nz, nx), F32), advection_dz=np.ones((ny, nz, nx), F32),
                 z=np.zeros((ny, nz, nx), F32), species={"qv": q}, dt=1.0)
     return case
+
+
+# ------------------------------------------------- on-device generation
+def device_member(nx: int, ny: int, nz: int, seed: int, device: int = 0, dx: float = 4000.0,
+                  dz: float = 500.0, species=ALL12):
+    """A config-1-style domain generated directly in GPU memory with torch
+    (for served requests, whose inputs must appear in milliseconds): Gaussian
+    ridge, Gal-Chen jacobians, uniform westerly with seeded noise, w from
+    discrete continuity, qv/theta profiles and clustered lognormal
+    hydrometeors with ~70 % zeros.  Returns (dict of float32 CUDA tensors in
+    the Fortran layout of Case, dt)."""
+    import torch
+    g = torch.Generator(device=f"cuda:{device}")
+    g.manual_seed(int(seed))
+    dev = torch.device("cuda", device)
+    f32 = torch.float32
+    r = lambda *s: torch.rand(*s, generator=g, device=dev, dtype=f32)
+    n = lambda *s: torch.randn(*s, generator=g, device=dev, dtype=f32)
+    x = (torch.arange(nx, device=dev, dtype=f32) - (nx - 1) / 2.0) * dx
+    y = (torch.arange(ny, device=dev, dtype=f32) - (ny - 1) / 2.0) * dx
+    h = float(800.0 + 1200.0 * r(1).item())
+    terrain = h * torch.exp(-(x[None, :] ** 2 + y[:, None] ** 2) / 20000.0 ** 2)
+    H = dz * nz
+    jac1 = (H - terrain) / H
+    jac = jac1[:, None, :].expand(ny, nz, nx).contiguous()
+    dzi = dz * jac
+    ju = torch.empty(ny, nz, nx + 1, device=dev, dtype=f32)
+    ju[:, :, 0] = jac[:, :, 0]
+    ju[:, :, nx] = jac[:, :, nx - 1]
+    ju[:, :, 1:nx] = (jac[:, :, 1:] + jac[:, :, :-1]) / 2
+    jv = torch.empty(ny + 1, nz, nx, device=dev, dtype=f32)
+    jv[0] = jac[0]
+    jv[ny] = jac[ny - 1]
+    jv[1:ny] = (jac[1:] + jac[:-1]) / 2
+    jw = torch.empty(ny, nz, nx, device=dev, dtype=f32)
+    jw[:, nz - 1] = jac[:, nz - 1]
+    jw[:, :nz - 1] = (dzi[:, :-1] * jac[:, :-1] + dzi[:, 1:] * jac[:, 1:]) / (dzi[:, :-1] + dzi[:, 1:])
+    adz = torch.full((ny, nz, nx), dz, device=dev, dtype=f32)
+    U = float(8.0 + 4.0 * r(1).item())
+    u = U + 0.02 * U * n(ny, nz, nx + 1)
+    v = 0.02 * U * n(ny + 1, nz, nx)
+    div = ((u * ju)[:, :, 1:] - (u * ju)[:, :, :-1] + (v * jv)[1:] - (v * jv)[:-1]) / dx
+    w = torch.empty(ny, nz, nx, device=dev, dtype=f32)
+    w[:, 0] = (0 - div[:, 0] * adz[:, 0]) / jw[:, 0]
+    for k in range(1, nz):
+        w[:, k] = (w[:, k - 1] * jw[:, k - 1] - div[:, k] * adz[:, k]) / jw[:, k]
+    zc = terrain[:, None, :] + torch.cumsum(dzi, dim=1) - dzi / 2
+    rho = 1.225 * torch.exp(-zc / 8500.0)
+
+    def clustered(frac=0.7, median=1e-4):
+        c = n(ny // 8 + 2, nz // 4 + 2, nx // 8 + 2)
+        c = c.repeat_interleave(8, 0).repeat_interleave(4, 1).repeat_interleave(8, 2)[:ny, :nz, :nx]
+        thr = torch.quantile(c.reshape(-1)[:: max(1, c.numel() // 100000)], frac)
+        return torch.where(c > thr, median * torch.exp(n(ny, nz, nx)), torch.zeros((), device=dev))
+
+    out = {"u": u, "v": v, "w": w, "density": rho, "jacobian": jac, "jacobian_u": ju, "jacobian_v": jv,
+           "jacobian_w": jw, "advection_dz": adz}
+    masses = {}
+    sp = {}
+    for nm in species:
+        if nm == "qv":
+            sp[nm] = 0.010 * torch.exp(-zc / 2500.0) * (1 + 0.01 * n(ny, nz, nx))
+        elif nm == "theta":
+            sp[nm] = 300.0 * torch.exp(1e-4 * zc / 9.81)
+        elif nm in HYDROMETEORS:
+            masses[nm] = clustered()
+            sp[nm] = masses[nm]
+    for nm in species:
+        if nm in NUMBERS:
+            m = masses.get(NUMBERS[nm])
+            if m is None:
+                m = clustered()
+            sp[nm] = torch.where(m > 0, 1e5 * torch.exp(n(ny, nz, nx)), torch.zeros((), device=dev))
+    out["species"] = {nm: sp[nm].to(f32).contiguous() for nm in species}
+    for k in list(out):
+        if k != "species":
+            out[k] = out[k].to(f32).contiguous()
+    return out, 20.0
