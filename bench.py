@@ -529,7 +529,7 @@ def run_served(args):
         srv.submit(r)
     clocks = ClockSampler(local)
     clocks.start()
-    srv.t0 = time.perf_counter()
+    srv.start_clock()
     srv.run()
     clk = clocks.stop()
     rep = srv.report()

@@ -1016,6 +1016,13 @@ struct icar_adv_batch {
     size_t off_up = 0, off_nblk = 0, off_f = 0, off_counter = 0;
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int stable_steps = 0;  // steps since the last table rebuild; graphs are captured once it reaches 2
+    // pinned staging for the table uploads, two sets used in turn; an event
+    // marks when a set's last upload has been consumed by the stream
+    char *stage[2] = {nullptr, nullptr};
+    size_t stage_cap[2] = {0, 0};
+    cudaEvent_t stage_done[2] = {nullptr, nullptr};
+    int stage_turn = 0;
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
     int64_t steps = 0;
@@ -1052,9 +1059,9 @@ template <class T>
 int grow(icar_adv_batch_t *b, T *&p, size_t &cap, size_t n)
 {
     if (n <= cap && p) return ICAR_ADV_OK;
-    if (p) cudaFree(p);
+    if (p) cudaFree(p);  // synchronises the device: queued launches may still read it
     p = nullptr;
-    size_t c = std::max<size_t>(n, 16);
+    size_t c = std::max<size_t>(n + n / 2, 16);
     BCUDA(b, cudaMalloc(&p, c * sizeof(T)));
     cap = c;
     return ICAR_ADV_OK;
@@ -1164,19 +1171,41 @@ int build_tables(icar_adv_batch_t *b)
     if ((e = grow(b, b->d_ints, b->ints_cap, ints.size()))) return e;
     if ((e = grow(b, b->d_pairs, b->pairs_cap, std::max<size_t>(pairs.size(), 1)))) return e;
     if ((e = grow(b, b->d_items, b->items_cap, std::max<size_t>(items.size(), 1)))) return e;
-    BCUDA(b, cudaMemcpyAsync(b->d_mem[0], mem[0].data(), sizeof(icar::BatchMember) * std::max(M, 1),
-                             cudaMemcpyHostToDevice, b->stream));
-    BCUDA(b, cudaMemcpyAsync(b->d_mem[1], mem[1].data(), sizeof(icar::BatchMember) * std::max(M, 1),
-                             cudaMemcpyHostToDevice, b->stream));
-    BCUDA(b, cudaMemcpyAsync(b->d_ints, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice, b->stream));
-    if (!pairs.empty())
-        BCUDA(b, cudaMemcpyAsync(b->d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice,
-                                 b->stream));
-    if (!items.empty())
-        BCUDA(b, cudaMemcpyAsync(b->d_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice,
-                                 b->stream));
-    // the host vectors die here: finish the copies first
-    BCUDA(b, cudaStreamSynchronize(b->stream));
+    // Upload through pinned staging, stream-ordered after every launch already
+    // queued (those still read the old tables), without a host sync.  Two
+    // staging sets alternate; a set is reused only after its previous upload
+    // has been consumed.
+    const size_t bm = sizeof(icar::BatchMember) * std::max(M, 1);
+    const size_t seg[5] = {bm, bm, sizeof(int) * ints.size(), sizeof(int2) * pairs.size(),
+                           sizeof(int4) * items.size()};
+    size_t off[5], total = 0;
+    for (int i = 0; i < 5; i++) {
+        off[i] = total;
+        total += (seg[i] + 255) / 256 * 256;
+    }
+    const int t = b->stage_turn;
+    if (b->stage_done[t]) BCUDA(b, cudaEventSynchronize(b->stage_done[t]));
+    else BCUDA(b, cudaEventCreateWithFlags(&b->stage_done[t], cudaEventDisableTiming));
+    if (total > b->stage_cap[t]) {
+        if (b->stage[t]) cudaFreeHost(b->stage[t]);
+        b->stage[t] = nullptr;
+        b->stage_cap[t] = 0;
+        BCUDA(b, cudaHostAlloc((void **)&b->stage[t], total * 3 / 2, cudaHostAllocDefault));
+        b->stage_cap[t] = total * 3 / 2;
+    }
+    char *st = b->stage[t];
+    memcpy(st + off[0], mem[0].data(), seg[0]);
+    memcpy(st + off[1], mem[1].data(), seg[1]);
+    memcpy(st + off[2], ints.data(), seg[2]);
+    if (seg[3]) memcpy(st + off[3], pairs.data(), seg[3]);
+    if (seg[4]) memcpy(st + off[4], items.data(), seg[4]);
+    BCUDA(b, cudaMemcpyAsync(b->d_mem[0], st + off[0], seg[0], cudaMemcpyHostToDevice, b->stream));
+    BCUDA(b, cudaMemcpyAsync(b->d_mem[1], st + off[1], seg[1], cudaMemcpyHostToDevice, b->stream));
+    BCUDA(b, cudaMemcpyAsync(b->d_ints, st + off[2], seg[2], cudaMemcpyHostToDevice, b->stream));
+    if (seg[3]) BCUDA(b, cudaMemcpyAsync(b->d_pairs, st + off[3], seg[3], cudaMemcpyHostToDevice, b->stream));
+    if (seg[4]) BCUDA(b, cudaMemcpyAsync(b->d_items, st + off[4], seg[4], cudaMemcpyHostToDevice, b->stream));
+    BCUDA(b, cudaEventRecord(b->stage_done[t], b->stream));
+    b->stage_turn ^= 1;
     b->ctas = std::min(std::max(b->n_items, 1), icar::batch_corr_max_ctas(b->shape, b->fct, b->nsm));
     b->tables_dirty = false;
     return ICAR_ADV_OK;
@@ -1279,7 +1308,13 @@ int icar_adv_batch_remove(icar_adv_batch_t *b, icar_adv_t *h)
     auto it = std::find(b->members.begin(), b->members.end(), h);
     if (it == b->members.end()) return bfail(b, ICAR_ADV_BAD_ARG, "domain is not a member of this batch");
     cudaSetDevice(b->device);
-    cudaStreamSynchronize(b->stream);
+    // the member's own stream waits for every batch launch already queued
+    // (they may still read its buffers); no host synchronisation
+    cudaEvent_t ev = nullptr;
+    BCUDA(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    BCUDA(b, cudaEventRecord(ev, b->stream));
+    BCUDA(b, cudaStreamWaitEvent(h->own_stream, ev, 0));
+    cudaEventDestroy(ev);
     b->dts.erase(b->dts.begin() + (it - b->members.begin()));
     b->members.erase(it);
     h->batch = nullptr;
@@ -1322,15 +1357,24 @@ int icar_adv_batch_step(icar_adv_batch_t *b)
         b->parity = 0;
         if ((e = build_tables(b))) return e;
         b->graph_dirty = true;
+        b->stable_steps = 0;
     }
-    if (b->graph_dirty && (e = build_graphs(b))) return e;
+    // while membership keeps changing (serving), launch directly; capture the
+    // step in graphs once the same tables have served two steps
+    if (b->graph_dirty && b->stable_steps >= 2 && (e = build_graphs(b))) return e;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (b->profiling) {
         cudaEventCreate(&ev0);
         cudaEventCreate(&ev1);
         cudaEventRecord(ev0, b->stream);
     }
-    BCUDA(b, cudaGraphLaunch(b->exec[b->parity], b->stream));
+    if (!b->graph_dirty) {
+        BCUDA(b, cudaGraphLaunch(b->exec[b->parity], b->stream));
+    } else {
+        enqueue_step(b, b->parity, b->stream);
+        BCUDA(b, cudaGetLastError());
+    }
+    b->stable_steps++;
     if (b->profiling) {
         cudaEventRecord(ev1, b->stream);
         b->events.emplace_back(ev0, ev1);
@@ -1423,6 +1467,10 @@ int icar_adv_batch_destroy(icar_adv_batch_t *b)
     if (b->d_ints) cudaFree(b->d_ints);
     if (b->d_pairs) cudaFree(b->d_pairs);
     if (b->d_items) cudaFree(b->d_items);
+    for (int t = 0; t < 2; t++) {
+        if (b->stage[t]) cudaFreeHost(b->stage[t]);
+        if (b->stage_done[t]) cudaEventDestroy(b->stage_done[t]);
+    }
     cudaStreamDestroy(b->stream);
     delete b;
     return ICAR_ADV_OK;

@@ -89,9 +89,12 @@ class Server:
         self.max_slots = max_slots
         self.options = options or Options()
         self.keep_results = keep_results
+        import torch
         self.batch = Batch(device)
-        if stream is not None:
-            self.batch.set_stream(stream)
+        # the batch runs on this stream; completion times come from events on it
+        self.stream = torch.cuda.Stream(device) if stream is None else torch.cuda.ExternalStream(stream, device)
+        self.batch.set_stream(self.stream.cuda_stream)
+        self._ev0 = None
         self.queue: collections.deque[Request] = collections.deque()
         self.live: list[_Live] = []
         self.used = 0
@@ -100,6 +103,8 @@ class Server:
         self.peak_used = 0
         self.peak_live = 0
         self.steps = 0
+        self.graveyard: list = []
+        self.flush_every = 16
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -143,14 +148,38 @@ class Server:
             self.batch.sync()
             req.result = {k: t.cpu().numpy().reshape(req.ny, req.nz, req.nx) for k, t in out.items()}
         self.batch.remove(lv.dom)
-        lv.dom.close()
+        # freeing device memory synchronises the device, so retired domains
+        # are destroyed in bulk (their memory stays counted until then)
+        self.graveyard.append((lv.dom, req.footprint))
+        if len(self.graveyard) >= self.flush_every or (self.queue and self.used + self.queue[0].footprint > self.budget):
+            self._flush_graveyard()
         req.finished = self.now()
-        self.used -= req.footprint
         self.done.append(req)
 
+    def _flush_graveyard(self) -> None:
+        for dom, fp in self.graveyard:
+            dom.close()
+            self.used -= fp
+        self.graveyard.clear()
+
     # -- loop ---------------------------------------------------------------
+    def start_clock(self) -> None:
+        """t = 0 of the server clock, matched to an event on the batch stream."""
+        import torch
+        self.stream.synchronize()
+        self._ev0 = torch.cuda.Event(enable_timing=True)
+        self._ev0.record(self.stream)
+        self._ev0.synchronize()
+        self.t0 = time.perf_counter()
+
     def run(self, max_wall: float | None = None) -> None:
-        """Serve until every submitted request is done (or max_wall seconds)."""
+        """Serve until every submitted request is done (or max_wall seconds).
+        The host never waits for the device except to download kept results
+        and to free retired domains in bulk; a request's completion time is
+        read from an event recorded after its last step."""
+        import torch
+        if self._ev0 is None:
+            self.start_clock()
         while self.queue or self.live:
             if max_wall is not None and self.now() > max_wall:
                 break
@@ -167,10 +196,19 @@ class Server:
                 if lv.remaining == 0:
                     finished.append(lv)
             if finished:
-                self.batch.sync()          # the finishing step must be complete
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(self.stream)
                 for lv in finished:
                     self.live.remove(lv)
+                    lv.req._done_event = ev
                     self._retire(lv)
+        self._flush_graveyard()
+        for r in self.done:
+            ev = getattr(r, "_done_event", None)
+            if ev is not None:
+                ev.synchronize()
+                r.finished = self._ev0.elapsed_time(ev) / 1e3
+                r._done_event = None
 
     def report(self) -> dict:
         done = [r for r in self.done if r.finished is not None]
