@@ -154,9 +154,7 @@ constexpr int S_W = 13;           // W' = W_m/dz, 3 slots
 constexpr int S_G = 16;           // G = J*rho, 3 slots
 constexpr int S_U2 = 19, S_V2 = 20;  // unlimited pseudo-velocities of level t
 constexpr int S_BXI = 21, S_BXO = 22, S_BYI = 23, S_BYO = 24;
-constexpr int S_U2L = 25;         // 2 ring slots
-constexpr int S_V2L = 27;         // 2 ring slots
-constexpr int NPLANES = 29;
+constexpr int NPLANES = 25;
 template <class SH>
 constexpr size_t smem_bytes() { return (size_t)NPLANES * SH::PLANE * sizeof(float); }
 }  // namespace mpf
@@ -203,6 +201,16 @@ __device__ __forceinline__ void load_plane(float *dst, const float *__restrict__
 // branch costs more than the divisions it skips in mixed warps).
 __device__ __forceinline__ float div0(float n, float d) { return n / d; }
 
+// Limited pseudo-velocity at a face (flux_limiter, adv_mpdata_FCT_core.f90):
+// flow towards +x/+y/+z takes beta_in of the cell after the face and
+// beta_out of the cell before it, flow the other way the opposite pair.
+__device__ __forceinline__ float fct_limit(float u, float bin_r, float bout_l, float bin_l, float bout_r)
+{
+    if (u > 0.0f) return fminf(fminf(1.0f, bin_r), bout_l) * u;
+    if (u < 0.0f) return fminf(fminf(1.0f, bin_l), bout_r) * u;
+    return u;
+}
+
 // One 28 x TY column tile of one species: the z-march described at the top
 // of this file.  i0 is the first output column (i0-2 a multiple of 4), j0
 // the first output row; sm is the CTA's dynamic shared memory.
@@ -240,11 +248,13 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
     // r_q1dn / r_q0dn: q1 and q0 one level below the level being limited;
     // r_q1dd: q1 two levels below (the level under the corrective pass).
     float r_fz[RPW], r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_w2l[RPW], r_q1dn[RPW], r_q0dn[RPW], r_q1dd[RPW];
-    float r_G[RPW], r_DJR[RPW];
+    // r_part: the horizontal part of the corrective pass one level below.
+    float r_part[RPW], r_DJR[RPW];
 #pragma unroll
     for (int rr = 0; rr < RPW; rr++) {
         r_fz[rr] = r_w2[rr] = r_bzi[rr] = r_bzo[rr] = r_w2l[rr] = r_q1dn[rr] = r_q0dn[rr] = r_q1dd[rr] = 0.0f;
-        r_G[rr] = r_DJR[rr] = 1.0f;
+        r_part[rr] = 0.0f;
+        r_DJR[rr] = 1.0f;
     }
 
     for (int t = 0; t <= nz; t++) {
@@ -271,7 +281,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
         const int sGc = S_G + t % 3, sGp = S_G + (t + 1) % 3;
         const bool kint = t > 0 && t < nz - 1;
 
-        float n_fz[RPW], n_w2[RPW], n_bzi[RPW] = {}, n_bzo[RPW] = {}, n_w2l[RPW];
+        float n_fz[RPW], n_w2[RPW], n_bzi[RPW] = {}, n_bzo[RPW] = {}, n_w2l[RPW], n_part[RPW];
         if (haveA) {
             // ---------------- A1: u2, v2 at level t; w2 at the top of t --------
             for (int r = warp; r < TY; r += NW) {  // u2 faces x in [-1, TX+1] -> lx 1..31
@@ -468,71 +478,57 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                 }
                 __syncthreads();
             }
-            // ---------------- A3: limited u2, v2 at level t -------------------
-            float *u2l = P(S_U2L + (t & 1)), *v2l = P(S_V2L + (t & 1));
-            for (int r = warp; r < TY; r += NW) {  // faces x in [0, TX] -> lx 2..TX+2
-                const int ly = r + 2, lx = lane;
-                if (lx >= 2 && lx <= TX + 2) {
-                    float u = AT(S_U2, lx, ly);
-                    if (FCT) {
-                        if (u > 0.0f)
-                            u = fminf(fminf(1.0f, AT(S_BXI, lx, ly)), AT(S_BXO, lx - 1, ly)) * u;
-                        else if (u < 0.0f)
-                            u = fminf(fminf(1.0f, AT(S_BXI, lx - 1, ly)), AT(S_BXO, lx, ly)) * u;
-                    }
-                    u2l[ly * PW + lx] = u;
-                }
-            }
-            for (int r = warp; r < TY + 1; r += NW) {  // faces y in [0, TY] -> ly 2..TY+2
-                const int ly = r + 2, lx = lane;
-                if (lx >= 2 && lx < TX + 2) {
-                    float v = AT(S_V2, lx, ly);
-                    if (FCT) {
-                        if (v > 0.0f)
-                            v = fminf(fminf(1.0f, AT(S_BYI, lx, ly)), AT(S_BYO, lx, ly - 1)) * v;
-                        else if (v < 0.0f)
-                            v = fminf(fminf(1.0f, AT(S_BYI, lx, ly - 1)), AT(S_BYO, lx, ly)) * v;
-                    }
-                    v2l[ly * PW + lx] = v;
-                }
-            }
-            // limited w2 at the top face of level t-1
+            // ------- B1: horizontal part of the corrective pass at level t --------
+            // The limited face velocities are formed here from the unlimited
+            // ones and the limiter terms of the two cells beside each face;
+            // the result waits in a register for the vertical part (B2).
 #pragma unroll
             for (int rr = 0; rr < RPW; rr++) {
-                float w = r_w2[rr];
-                if (FCT && t >= 1) {
-                    if (w > 0.0f)
-                        w = fminf(fminf(1.0f, n_bzi[rr]), r_bzo[rr]) * w;
-                    else if (w < 0.0f)
-                        w = fminf(fminf(1.0f, r_bzi[rr]), n_bzo[rr]) * w;
+                const int ly = warp + NW * rr + 2, lx = lane + 2;
+                const int i = i0 - 2 + lx, j = j0 - 2 + ly;
+                n_part[rr] = 0.0f;
+                if (lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
+                    float uw = AT(S_U2, lx, ly), ue = AT(S_U2, lx + 1, ly);
+                    float vs = AT(S_V2, lx, ly), vn = AT(S_V2, lx, ly + 1);
+                    if (FCT) {
+                        const float bxi_c = AT(S_BXI, lx, ly), bxo_c = AT(S_BXO, lx, ly);
+                        const float byi_c = AT(S_BYI, lx, ly), byo_c = AT(S_BYO, lx, ly);
+                        uw = fct_limit(uw, bxi_c, AT(S_BXO, lx - 1, ly), AT(S_BXI, lx - 1, ly), bxo_c);
+                        ue = fct_limit(ue, AT(S_BXI, lx + 1, ly), bxo_c, bxi_c, AT(S_BXO, lx + 1, ly));
+                        vs = fct_limit(vs, byi_c, AT(S_BYO, lx, ly - 1), AT(S_BYI, lx, ly - 1), byo_c);
+                        vn = fct_limit(vn, AT(S_BYI, lx, ly + 1), byo_c, byi_c, AT(S_BYO, lx, ly + 1));
+                    }
+                    const float qc = AT(sQc, lx, ly);
+                    const float fe = flux1(qc, AT(sQc, lx + 1, ly), ue);
+                    const float fw = flux1(AT(sQc, lx - 1, ly), qc, uw);
+                    const float f3 = flux1(qc, AT(sQc, lx, ly + 1), vn);
+                    const float f4 = flux1(AT(sQc, lx, ly - 1), qc, vs);
+                    n_part[rr] = qc - div0((fe - fw) + (f3 - f4), AT(sGc, lx, ly));
                 }
+                // limited w2 at the top face of level t-1
+                float w = r_w2[rr];
+                if (FCT && t >= 1) w = fct_limit(w, n_bzi[rr], r_bzo[rr], r_bzi[rr], n_bzo[rr]);
                 n_w2l[rr] = w;
             }
         } else {
 #pragma unroll
             for (int rr = 0; rr < RPW; rr++) {
                 n_w2l[rr] = 0.0f;  // top face of the model: w2(kme) = 0
-                n_fz[rr] = n_w2[rr] = n_bzi[rr] = n_bzo[rr] = 0.0f;
+                n_fz[rr] = n_w2[rr] = n_bzi[rr] = n_bzo[rr] = n_part[rr] = 0.0f;
             }
         }
 
-        // ---------------- B: corrective donor-cell pass at level t-1 ----------
+        // ---------------- B2: finish the corrective pass at level t-1 ----------
         if (t >= 1) {
             const int L = t - 1;
-            const int sQL = sQm;  // q1 plane of level t-1
-            const float *u2l = P(S_U2L + (L & 1)), *v2l = P(S_V2L + (L & 1));
 #pragma unroll
             for (int rr = 0; rr < RPW; rr++) {
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
                 const int i = i0 - 2 + lx, j = j0 - 2 + ly;
                 if (lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
-                    const float qc = AT(sQL, lx, ly);
-                    const float fe = flux1(qc, AT(sQL, lx + 1, ly), u2l[ly * PW + lx + 1]);
-                    const float fw = flux1(AT(sQL, lx - 1, ly), qc, u2l[ly * PW + lx]);
-                    const float f3 = flux1(qc, AT(sQL, lx, ly + 1), v2l[(ly + 1) * PW + lx]);
-                    const float f4 = flux1(AT(sQL, lx, ly - 1), qc, v2l[ly * PW + lx]);
-                    float val = qc - div0((fe - fw) + (f3 - f4), r_G[rr]);
+                    const float qc = r_q1dn[rr];
                     const float wtop = n_w2l[rr], wbot = r_w2l[rr];
+                    float val = r_part[rr];
                     if (L > 0 && L < nz - 1) {
                         const float f5t = flux1(qc, AT(sQc, lx, ly), wtop);
                         const float f5b = flux1(r_q1dd[rr], qc, wbot);
@@ -563,7 +559,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                 r_bzi[rr] = n_bzi[rr];
                 r_bzo[rr] = n_bzo[rr];
                 r_w2l[rr] = n_w2l[rr];
-                r_G[rr] = AT(sGc, lx, ly);
+                r_part[rr] = n_part[rr];
                 r_DJR[rr] = DJR[ix(g, i, t, j)];
             }
         }
