@@ -180,22 +180,53 @@ __device__ __forceinline__ float fct_beta(float num, float den)
     return num / den;
 }
 
-// Asynchronously copy level `lev` of a 3-D field into a plane slot, in
-// 16-byte chunks: the plane starts at x = i0-2, a multiple of 4, so every
+// Asynchronous copies of one level of a 3-D field into a plane slot, in
+// 16-byte chunks.  The plane starts at x = i0-2, a multiple of 4, so every
 // chunk is either wholly inside a row's pitch (valid cells, or the zero
-// padding past nx) or wholly outside the field and zero-filled.  ey is the
-// y extent of the field (ny, or ny+1 for y-face fields).
+// padding past nx) or wholly outside the field and zero-filled.  Chunk
+// e = tid + c*NT covers x from i0-2+4*(e%8) in row j0-2+e/8; its source
+// offset at level 0 and whether it lies inside a cell field (rows < ny) or
+// a y-face field (rows <= ny) are fixed for the whole tile, so copying a
+// level costs one add and one cp.async per chunk.
 template <class SH>
-__device__ __forceinline__ void load_plane(float *dst, const float *__restrict__ src, const Geo &g, int lev, int i0,
-                                           int j0, int ey)
-{
-    for (int e = threadIdx.x; e < (mpf::PW / 4) * SH::PH; e += SH::NT) {
-        const int cx = e % (mpf::PW / 4), ly = e / (mpf::PW / 4);
-        const int i = i0 - 2 + 4 * cx, j = j0 - 2 + ly;
-        const bool ok = i >= 0 && i < g.P && j >= 0 && j < ey;
-        cp_async16(dst + ly * mpf::PW + 4 * cx, ok ? src + ix(g, i, lev, j) : src, ok);
+struct PlaneLoader {
+    static constexpr int NCH = ((mpf::PW / 4) * SH::PH + SH::NT - 1) / SH::NT;
+    size_t off[NCH];
+    int dst[NCH];
+    unsigned okc, okv;
+    size_t lstride;
+    __device__ __forceinline__ PlaneLoader(const Geo &g, int i0, int j0) : okc(0u), okv(0u), lstride((size_t)g.P)
+    {
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            const int e = threadIdx.x + c * SH::NT;
+            dst[c] = -1;
+            off[c] = 0;
+            if (e < (mpf::PW / 4) * SH::PH) {
+                const int cx = e % (mpf::PW / 4), ly = e / (mpf::PW / 4);
+                const int i = i0 - 2 + 4 * cx, j = j0 - 2 + ly;
+                dst[c] = ly * mpf::PW + 4 * cx;
+                const bool in = i >= 0 && i < g.P && j >= 0;
+                if (in && j < g.ny) okc |= 1u << c;
+                if (in && j <= g.ny) {
+                    okv |= 1u << c;
+                    off[c] = (size_t)i + (size_t)g.P * g.nz * j;
+                }
+            }
+        }
     }
-}
+    __device__ __forceinline__ void load(float *plane, const float *__restrict__ src, int lev, bool yface) const
+    {
+        const unsigned ok = yface ? okv : okc;
+        const size_t lo = (size_t)lev * lstride;
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+            if (dst[c] < 0) continue;
+            const bool v = (ok >> c) & 1u;
+            cp_async16(plane + dst[c], v ? src + off[c] + lo : src, v);
+        }
+    }
+};
 
 // IEEE-rounded quotient (a zero-numerator shortcut was measured slower: the
 // branch costs more than the divisions it skips in mixed warps).
@@ -230,18 +261,19 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
     auto P = [&](int slot) { return sm + (size_t)slot * PLANE; };
 #define AT(slot, lx, ly) sm[(size_t)(slot) * PLANE + (ly) * PW + (lx)]
 
+    const PlaneLoader<SH> pl(g, i0, j0);
     // ---- prologue: levels 0 and 1 of everything the first iteration reads
-    load_plane<SH>(P(S_Q1 + 0), q1g, g, 0, i0, j0, ny);
-    load_plane<SH>(P(S_Q0 + 0), q0g, g, 0, i0, j0, ny);
-    load_plane<SH>(P(S_U + 0), Um, g, 0, i0, j0, ny);
-    load_plane<SH>(P(S_V + 0), Vm, g, 0, i0, j0, ny + 1);
-    load_plane<SH>(P(S_W + 0), Wp, g, 0, i0, j0, ny);
-    load_plane<SH>(P(S_G + 0), Gc, g, 0, i0, j0, ny);
-    load_plane<SH>(P(S_Q1 + 1), q1g, g, 1, i0, j0, ny);
-    load_plane<SH>(P(S_Q0 + 1), q0g, g, 1, i0, j0, ny);
-    load_plane<SH>(P(S_U + 1), Um, g, 1, i0, j0, ny);
-    load_plane<SH>(P(S_V + 1), Vm, g, 1, i0, j0, ny + 1);
-    load_plane<SH>(P(S_G + 1), Gc, g, 1, i0, j0, ny);
+    pl.load(P(S_Q1 + 0), q1g, 0, false);
+    pl.load(P(S_Q0 + 0), q0g, 0, false);
+    pl.load(P(S_U + 0), Um, 0, false);
+    pl.load(P(S_V + 0), Vm, 0, true);
+    pl.load(P(S_W + 0), Wp, 0, false);
+    pl.load(P(S_G + 0), Gc, 0, false);
+    pl.load(P(S_Q1 + 1), q1g, 1, false);
+    pl.load(P(S_Q0 + 1), q0g, 1, false);
+    pl.load(P(S_U + 1), Um, 1, false);
+    pl.load(P(S_V + 1), Vm, 1, true);
+    pl.load(P(S_G + 1), Gc, 1, false);
     cp_async_commit();
 
     // per-output-cell z state (two output rows per warp)
@@ -263,13 +295,13 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
         __syncthreads();
         // prefetch the levels the next iteration adds: q1/q0/U/V/G at t+2, W' at t+1
         if (t + 2 < nz) {
-            load_plane<SH>(P(S_Q1 + ((t + 2) & 3)), q1g, g, t + 2, i0, j0, ny);
-            load_plane<SH>(P(S_Q0 + (t + 2) % 3), q0g, g, t + 2, i0, j0, ny);
-            load_plane<SH>(P(S_U + (t + 2) % 3), Um, g, t + 2, i0, j0, ny);
-            load_plane<SH>(P(S_V + (t + 2) % 3), Vm, g, t + 2, i0, j0, ny + 1);
-            load_plane<SH>(P(S_G + (t + 2) % 3), Gc, g, t + 2, i0, j0, ny);
+            pl.load(P(S_Q1 + ((t + 2) & 3)), q1g, t + 2, false);
+            pl.load(P(S_Q0 + (t + 2) % 3), q0g, t + 2, false);
+            pl.load(P(S_U + (t + 2) % 3), Um, t + 2, false);
+            pl.load(P(S_V + (t + 2) % 3), Vm, t + 2, true);
+            pl.load(P(S_G + (t + 2) % 3), Gc, t + 2, false);
         }
-        if (t + 1 < nz) load_plane<SH>(P(S_W + (t + 1) % 3), Wp, g, t + 1, i0, j0, ny);
+        if (t + 1 < nz) pl.load(P(S_W + (t + 1) % 3), Wp, t + 1, false);
         cp_async_commit();
 
         const bool haveA = t < nz;
