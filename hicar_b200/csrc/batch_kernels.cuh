@@ -127,49 +127,19 @@ __global__ void k_batch_prep(const BatchMember *__restrict__ mem, const int *__r
     }
 }
 
-// prefix over members of S * ceil(nx*nz*ny/256) blocks; nblk[m] = blocks per species
-__global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix,
-                               const int *__restrict__ nblk, int nmem)
+// prefix over members of ceil(nx*nz*ny/256) blocks; every species of a cell in one thread
+__global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix, int nmem)
 {
     const int mi = find_owner(prefix, nmem, blockIdx.x);
     const BatchMember &m = mem[mi];
     const Geo g = m.g;
-    const int local = blockIdx.x - prefix[mi];
-    const int s = local / nblk[mi];
-    const size_t t = (size_t)(local - s * nblk[mi]) * blockDim.x + threadIdx.x;
+    const size_t t = (size_t)(blockIdx.x - prefix[mi]) * blockDim.x + threadIdx.x;
     const int i = (int)(t % (size_t)g.nx);
     const size_t rest = t / (size_t)g.nx;
     const int k = (int)(rest % (size_t)g.nz);
     const int j = (int)(rest / (size_t)g.nz);
     if (j >= g.ny) return;
-    const float *__restrict__ qin = m.q0[s];
-    const size_t c = ix(g, i, k, j);
-    const float q0 = qin[c];
-    if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) {
-        m.q1[s][c] = q0;
-        m.out[s][c] = q0;
-        return;
-    }
-    const size_t sy = (size_t)g.P * g.nz, sz = (size_t)g.P;
-    const float *__restrict__ U = m.Um, *__restrict__ V = m.Vm, *__restrict__ W = m.Wm;
-    float fe = flux1(q0, qin[c + 1], U[c + 1]);
-    float fw = flux1(qin[c - 1], q0, U[c]);
-    float f3 = flux1(q0, qin[c + sy], V[c + sy]);
-    float f4 = flux1(qin[c - sy], q0, V[c]);
-    float val = q0 - ((fe - fw) + (f3 - f4)) / m.Gc[c];
-    const float djr = m.DJR[c];
-    if (k > 0 && k < g.nz - 1) {
-        float f5t = flux1(q0, qin[c + sz], W[c]);
-        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
-        val = val - (f5t - f5b) / djr;
-    } else if (k == 0) {
-        float f5t = flux1(q0, qin[c + sz], W[c]);
-        val = val - f5t / djr;
-    } else {
-        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
-        val = val - (q0 * W[c] - f5b) / djr;
-    }
-    m.q1[s][c] = val;
+    mp_upwind_at(g, i, k, j, m.q0, m.q1, m.out, m.S, m.Um, m.Vm, m.Wm, m.Gc, m.DJR);
 }
 
 // Persistent correction kernel: items are (member, species, i0, j0).

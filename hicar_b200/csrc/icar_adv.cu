@@ -579,8 +579,8 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
     }
     const size_t nc = (size_t)g.nx * g.nz * g.ny;
     if (S > 0) {
-        dim3 gu(blocks_for(nc, 256), S);
-        icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p, h->DJR.p);
+        icar::k_mp_upwind<<<blocks_for(nc, 256), 256, 0, h->stream>>>(g, sp, S, h->Um.p, h->Vm.p, h->Wm.p,
+                                                                      h->Gc.p, h->DJR.p);
         icar::mp_corr_launch(h->stream, h->mp_shape, g, sp, S, h->opts.mpdata_fct, h->Um.p, h->Vm.p, h->Wp.p,
                              h->Gc.p, h->DJR.p, h->dz.p);
     }
@@ -1006,14 +1006,14 @@ struct icar_adv_batch {
     // device tables and work lists
     icar::BatchMember *d_mem[2] = {nullptr, nullptr};
     size_t mem_cap = 0;
-    int *d_ints = nullptr;   // prep prefix | upwind prefix | upwind nblk | forcing prefix | counter
+    int *d_ints = nullptr;   // prep prefix | upwind prefix | forcing prefix | counter
     size_t ints_cap = 0;
     int2 *d_pairs = nullptr;
     size_t pairs_cap = 0;
     int4 *d_items = nullptr;
     size_t items_cap = 0;
     int n_prep = 0, n_up = 0, n_force = 0, n_pairs = 0, n_items = 0, ctas = 0;
-    size_t off_up = 0, off_nblk = 0, off_f = 0, off_counter = 0;
+    size_t off_up = 0, off_f = 0, off_counter = 0;
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int stable_steps = 0;  // steps since the last table rebuild; graphs are captured once it reaches 2
@@ -1111,7 +1111,7 @@ int build_tables(icar_adv_batch_t *b)
     std::vector<icar::BatchMember> mem[2];
     mem[0].resize(std::max(M, 1));
     mem[1].resize(std::max(M, 1));
-    std::vector<int> prep(M + 1, 0), up(M + 1, 0), nblk(std::max(M, 1), 0), fpre(1, 0);
+    std::vector<int> prep(M + 1, 0), up(M + 1, 0), fpre(1, 0);
     std::vector<int2> pairs;
     std::vector<int4> items;
     const int ty = icar::mp_shape_ty(b->shape);
@@ -1124,8 +1124,7 @@ int build_tables(icar_adv_batch_t *b)
         const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
         const size_t nc = (size_t)g.nx * g.nz * g.ny;
         prep[m + 1] = prep[m] + (int)((nf + 255) / 256);
-        nblk[m] = (int)((nc + 255) / 256);
-        up[m + 1] = up[m] + nblk[m] * h->desc.n_species;
+        up[m + 1] = up[m] + (h->desc.n_species > 0 ? (int)((nc + 255) / 256) : 0);
         for (int s = 0; s < h->desc.n_species; s++) {
             if (h->forcing[s].p && h->nzone > 0) {
                 pairs.push_back(make_int2(m, s));
@@ -1160,13 +1159,11 @@ int build_tables(icar_adv_batch_t *b)
         b->mem_cap = cap;
     }
     b->off_up = M + 1;
-    b->off_nblk = b->off_up + M + 1;
-    b->off_f = b->off_nblk + std::max(M, 1);
+    b->off_f = b->off_up + M + 1;
     b->off_counter = b->off_f + fpre.size();
     std::vector<int> ints(b->off_counter + 1, 0);
     std::copy(prep.begin(), prep.end(), ints.begin());
     std::copy(up.begin(), up.end(), ints.begin() + b->off_up);
-    std::copy(nblk.begin(), nblk.end(), ints.begin() + b->off_nblk);
     std::copy(fpre.begin(), fpre.end(), ints.begin() + b->off_f);
     if ((e = grow(b, b->d_ints, b->ints_cap, ints.size()))) return e;
     if ((e = grow(b, b->d_pairs, b->pairs_cap, std::max<size_t>(pairs.size(), 1)))) return e;
@@ -1220,7 +1217,7 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
         icar::k_batch_forcing<<<b->n_force, 256, 0, st>>>(mem, b->d_ints + b->off_f, b->d_pairs, b->n_pairs);
     if (b->n_prep > 0) icar::k_batch_prep<<<b->n_prep, 256, 0, st>>>(mem, b->d_ints, M);
     if (b->n_up > 0)
-        icar::k_batch_upwind<<<b->n_up, 256, 0, st>>>(mem, b->d_ints + b->off_up, b->d_ints + b->off_nblk, M);
+        icar::k_batch_upwind<<<b->n_up, 256, 0, st>>>(mem, b->d_ints + b->off_up, M);
     cudaMemsetAsync(b->d_ints + b->off_counter, 0, sizeof(int), st);
     if (b->n_items > 0)
         icar::batch_corr_launch(st, b->shape, b->ctas, b->fct, mem, b->d_items, b->n_items,
@@ -1578,7 +1575,7 @@ extern "C" int icar_adv_advect_noalloc(const icar_adv_noalloc_args *a)
         sp.q0[0] = a->q_in[s];
         sp.q1[0] = q1;
         sp.out[0] = a->q_out[s];
-        icar::k_mp_upwind<<<dim3(blocks_for(ncell, 256), 1), 256, 0, st>>>(g, sp, Um, Vm, Wm, Gc, DJR);
+        icar::k_mp_upwind<<<blocks_for(ncell, 256), 256, 0, st>>>(g, sp, 1, Um, Vm, Wm, Gc, DJR);
         icar::mp_corr_launch(st, 1, g, sp, 1, a->mpdata_fct ? 1 : 0, Um, Vm, Wp, Gc, DJR, a->advection_dz);
     }
     ce = cudaGetLastError();

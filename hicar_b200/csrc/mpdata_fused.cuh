@@ -5,8 +5,8 @@
 //                 U_m, V_m, W_m (mpdata_compute_wind) plus G = J*rho,
 //                 DJR = dz*J*rho and W' = W_m/dz, formed with exactly the
 //                 reference's operations so every later use is bit-identical.
-//   k_mp_upwind   donor-cell pass q0 -> q1 for every species in one launch;
-//                 also writes the untouched boundary ring of the output.
+//   k_mp_upwind   donor-cell pass q0 -> q1, every species of a cell in one
+//                 thread; also writes the untouched boundary ring of the output.
 //   k_mp_corr     antidiffusive pseudo-velocities, FCT limiter and the
 //                 corrective donor-cell pass, fused: one CTA owns a 28x16
 //                 column tile of one species and marches up the column,
@@ -88,46 +88,63 @@ struct SpeciesPtrs {
 };
 
 // --------------------------------------------------------------------------
-// donor-cell pass 1 for every species; boundary ring of `out` = q0
+// donor-cell pass 1 (upwind_advection, adv_mpdata.f90:43-103) for every
+// species of one cell; boundary ring of `out` = q0.  The winds and metric
+// terms of the cell are read once and reused for all its species.
 // --------------------------------------------------------------------------
-__global__ void k_mp_upwind(Geo g, SpeciesPtrs sp, const float *__restrict__ U, const float *__restrict__ V,
-                            const float *__restrict__ W, const float *__restrict__ Gc,
-                            const float *__restrict__ DJR)
+__device__ __forceinline__ void mp_upwind_at(const Geo &g, int i, int k, int j, const float *const *q0s,
+                                             float *const *q1s, float *const *outs, int S,
+                                             const float *__restrict__ U, const float *__restrict__ V,
+                                             const float *__restrict__ W, const float *__restrict__ Gc,
+                                             const float *__restrict__ DJR)
 {
-    const int s = blockIdx.y;
-    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (int)(t % (size_t)g.nx);
-    size_t rest = t / (size_t)g.nx;
-    const int k = (int)(rest % (size_t)g.nz);
-    const int j = (int)(rest / (size_t)g.nz);
-    if (j >= g.ny) return;
-    const float *__restrict__ qin = sp.q0[s];
     const size_t c = ix(g, i, k, j);
-    const float q0 = qin[c];
     if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) {
-        sp.q1[s][c] = q0;
-        sp.out[s][c] = q0;
+        for (int s = 0; s < S; s++) {
+            const float q0 = q0s[s][c];
+            q1s[s][c] = q0;
+            outs[s][c] = q0;
+        }
         return;
     }
     const size_t sy = (size_t)g.P * g.nz, sz = (size_t)g.P;
-    float fe = flux1(q0, qin[c + 1], U[c + 1]);
-    float fw = flux1(qin[c - 1], q0, U[c]);
-    float f3 = flux1(q0, qin[c + sy], V[c + sy]);
-    float f4 = flux1(qin[c - sy], q0, V[c]);
-    float val = q0 - ((fe - fw) + (f3 - f4)) / Gc[c];
-    const float djr = DJR[c];
-    if (k > 0 && k < g.nz - 1) {
-        float f5t = flux1(q0, qin[c + sz], W[c]);
-        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
-        val = val - (f5t - f5b) / djr;
-    } else if (k == 0) {
-        float f5t = flux1(q0, qin[c + sz], W[c]);
-        val = val - f5t / djr;
-    } else {
-        float f5b = flux1(qin[c - sz], q0, W[c - sz]);
-        val = val - (q0 * W[c] - f5b) / djr;
+    const float ue = U[c + 1], uw = U[c], vn = V[c + sy], vs = V[c];
+    const float wt = W[c], wb = k > 0 ? W[c - sz] : 0.0f;
+    const float G = Gc[c], djr = DJR[c];
+    const bool mid = k > 0 && k < g.nz - 1;
+    for (int s = 0; s < S; s++) {
+        const float *__restrict__ qin = q0s[s];
+        const float q0 = qin[c];
+        const float fe = flux1(q0, qin[c + 1], ue);
+        const float fw = flux1(qin[c - 1], q0, uw);
+        const float f3 = flux1(q0, qin[c + sy], vn);
+        const float f4 = flux1(qin[c - sy], q0, vs);
+        float val = q0 - ((fe - fw) + (f3 - f4)) / G;
+        if (mid) {
+            const float f5t = flux1(q0, qin[c + sz], wt);
+            const float f5b = flux1(qin[c - sz], q0, wb);
+            val = val - (f5t - f5b) / djr;
+        } else if (k == 0) {
+            const float f5t = flux1(q0, qin[c + sz], wt);
+            val = val - f5t / djr;
+        } else {
+            const float f5b = flux1(qin[c - sz], q0, wb);
+            val = val - (q0 * wt - f5b) / djr;
+        }
+        q1s[s][c] = val;
     }
-    sp.q1[s][c] = val;
+}
+
+__global__ void k_mp_upwind(Geo g, SpeciesPtrs sp, int S, const float *__restrict__ U, const float *__restrict__ V,
+                            const float *__restrict__ W, const float *__restrict__ Gc, const float *__restrict__ DJR)
+{
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)(t % (size_t)g.nx);
+    const size_t rest = t / (size_t)g.nx;
+    const int k = (int)(rest % (size_t)g.nz);
+    const int j = (int)(rest / (size_t)g.nz);
+    if (j >= g.ny) return;
+    mp_upwind_at(g, i, k, j, sp.q0, sp.q1, sp.out, S, U, V, W, Gc, DJR);
 }
 
 namespace mpf {
