@@ -44,12 +44,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="full_species",
-                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served"])
+                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large"])
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-duration", type=float, default=6.0)
     p.add_argument("--serve-steps-scale", type=float, default=0.1)
     p.add_argument("--members", type=int, default=64, help="ensemble size (ensemble workload)")
-    p.add_argument("--tile-shape", type=int, default=1, help="fused-kernel tile shape 0..3 (8/16/24/32 rows)")
+    p.add_argument("--tile-shape", default="auto", choices=["auto", "0", "1", "2", "3"],
+                   help="fused-kernel tile shape 0..3 (8/16/24/32 rows), or auto: chosen by hicar_b200.autotune")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
     p.add_argument("--quick", action="store_true",
@@ -214,6 +215,7 @@ def run_b200(args):
     adv_init(d, opts)
     if args.staged:
         d.use_staged_kernels(True)
+    launch = set_launch_shape(d, args)
     # a dedicated stream: the library and the timing events share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -311,6 +313,7 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
                        "kernel_path": "staged" if args.staged else "fused",
+                       "launch_shape": launch,
                        "l2": "inputs larger than L2 (12 fields x 42 MB per domain)",
                        "parallelism": f"replicas x{world}"},
             "roofline": rl,
@@ -324,6 +327,103 @@ def run_b200(args):
     d.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def set_launch_shape(d, args) -> dict:
+    """Tile shape and species group of the fused kernels for this domain."""
+    from hicar_b200 import autotune
+    if args.tile_shape == "auto" and not args.staged:
+        c = autotune.tune_and_apply(d, fct=True)
+        return {"tile_rows": c.rows, "species_group": c.species_group,
+                "chosen_by": "autotune: every shape and group timed on a synthetic domain of this grid shape"}
+    shape = 1 if args.tile_shape == "auto" else int(args.tile_shape)
+    d.set_launch_shape(shape, 0)
+    return {"tile_rows": autotune.TILE_ROWS[shape], "species_group": 0, "chosen_by": "--tile-shape"}
+
+
+# ------------------------------------------------------------ large domain
+LARGE_DESC = "large single domain 2048x2048x60, dx 250 m, fractal terrain up to 4000 m, 12 fields, dt 1 s"
+
+
+def run_large(args):
+    """The large single domain, generated on the device: the default launch
+    shape against the autotuned one (every tile shape and species group timed
+    on this domain itself; the state advances while they are timed)."""
+    import torch
+    from hicar_b200 import _lib as L, autotune, roofline, synth
+    from hicar_b200.advection import Domain, Options, advect
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    nx, ny, nz = 2048, 2048, 60
+    fields, dt = synth.device_config5(seed=3, nx=nx, ny=ny, nz=nz, device=local)
+    opts = Options()
+    d = Domain.create_on_device(fields, nx, ny, nz, 250.0, opts, device=local, forcing=True)
+    d._device_fields = None
+    del fields
+    torch.cuda.empty_cache()
+    lib = L.load()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
+    h = d.handle
+    S = len(d.adv_vars)
+    cs = nx * ny * nz * S
+
+    def step():
+        L.check(lib.icar_adv_step(h, C.c_double(dt), 0), h)
+
+    def timed(steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        L.check(lib.icar_adv_profile(h, 1), h)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        kms, kl, al, ps = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
+        L.check(lib.icar_adv_profile_read(h, C.byref(kms), C.byref(kl), C.byref(al), C.byref(ps)), h)
+        L.check(lib.icar_adv_profile(h, 0), h)
+        return e0.elapsed_time(e1), kms.value, ps.value, al.value
+
+    d.set_launch_shape(1, 0)
+    for _ in range(args.warmup):
+        step()
+    ms_plain, _, _, _ = timed(args.steps)
+    measured = {}
+    for shape in range(len(autotune.TILE_ROWS)):
+        for group in autotune.species_groups(S):
+            d.set_launch_shape(shape, group)
+            step()
+            measured[f"{shape}:{group}"] = timed(2)[0] / 2
+    best = min(measured, key=measured.get)
+    shape, group = (int(v) for v in best.split(":"))
+    d.set_launch_shape(shape, group)
+    step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    ms, kms, passes, launches = timed(args.steps)
+    clk = clocks.stop()
+    rl = roofline.species_pass(nx, ny, nz, S, kms, passes)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": cs * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (generated on the device)",
+            "config": {"workload": LARGE_DESC, "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
+                       "launch_shape": {"tile_rows": autotune.TILE_ROWS[shape], "species_group": group,
+                                        "chosen_by": "autotune: every combination timed on this domain"},
+                       "l2": "inputs larger than L2 (12 fields x 1 GB)"},
+            "plain": {"value": cs * args.steps / (ms_plain / 1e3), "ms_per_step": ms_plain / args.steps,
+                      "launch_shape": {"tile_rows": 16, "species_group": 0}},
+            "autotuned_over_plain": ms_plain / ms,
+            "autotune_ms_per_step": measured,
+            "device_bytes": d.device_bytes(),
+            "roofline": rl, "gpu_launches": int(launches), "clocks": clk}), flush=True)
+    d.close()
 
 
 # ------------------------------------------------------------ ensemble
@@ -416,9 +516,14 @@ def run_ensemble(args):
     # ---- batched: every member in one graph launch per step
     b = Batch(device=local)
     b.set_stream(stream.cuda_stream)
-    b.set_tile_shape(args.tile_shape)
     for d, c in zip(doms, cases):
         b.add(d, c.dt)
+    if args.tile_shape == "auto":
+        from hicar_b200 import autotune
+        shape = autotune.tune_batch(b)
+    else:
+        shape = int(args.tile_shape)
+        b.set_tile_shape(shape)
     for _ in range(args.warmup):
         b.step()
     clocks = ClockSampler(local)
@@ -488,7 +593,8 @@ def run_ensemble(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": ENSEMBLE_DESC, "members": len(cases), "cell_species_per_step": cs_step,
                        "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
-                       "tile_shape_rows": [8, 16, 24, 32][args.tile_shape],
+                       "tile_shape_rows": [8, 16, 24, 32][shape],
+                       "tile_shape_chosen_by": "autotune cost model" if args.tile_shape == "auto" else "--tile-shape",
                        "l2": "inputs larger than L2 (~6 GB of species per step)",
                        "parallelism": f"replicas x{world}"},
             "plain": {"value": plain_value, "steps": plain_steps, "ms_per_step": plain_ms / plain_steps,
@@ -551,6 +657,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "large":
+        run_large(args)
     else:
         run_b200(args)
 

@@ -96,12 +96,14 @@ _PROTOS = {
     "icar_adv_set_path": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_set_species_group": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "icar_adv_batch_destroy": (C.c_int, [C.c_void_p]),
     "icar_adv_batch_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
     "icar_adv_batch_remove": (C.c_int, [C.c_void_p, C.c_void_p]),
     "icar_adv_batch_set_dt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
     "icar_adv_batch_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_batch_set_species_group": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_step": (C.c_int, [C.c_void_p]),
     "icar_adv_batch_sync": (C.c_int, [C.c_void_p]),
     "icar_adv_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),

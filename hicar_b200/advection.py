@@ -243,6 +243,16 @@ class Domain:
         L.check(L.load().icar_adv_device_bytes(self.handle, C.byref(b)), self.handle)
         return int(b.value)
 
+    def set_launch_shape(self, tile_shape: int | None = None, species_group: int | None = None) -> None:
+        """Tile shape of the fused correction kernel (0..3 = 8/16/24/32 rows
+        per tile) and species per thread of its donor-cell pass (0 = all);
+        see hicar_b200.autotune.  Results do not depend on either."""
+        lib = L.load()
+        if tile_shape is not None:
+            L.check(lib.icar_adv_set_tile_shape(self.handle, int(tile_shape)), self.handle)
+        if species_group is not None:
+            L.check(lib.icar_adv_set_species_group(self.handle, int(species_group)), self.handle)
+
     def use_staged_kernels(self, staged: bool = True) -> None:
         L.check(L.load().icar_adv_set_path(self.handle, 1 if staged else 0), self.handle)
 

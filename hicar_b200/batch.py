@@ -51,6 +51,9 @@ class Batch:
     def set_tile_shape(self, shape: int) -> None:
         self._check(self._lib.icar_adv_batch_set_tile_shape(self._b, int(shape)), self._b)
 
+    def set_species_group(self, group: int) -> None:
+        self._check(self._lib.icar_adv_batch_set_species_group(self._b, int(group)), self._b)
+
     def set_stream(self, cuda_stream: int) -> None:
         self._check(self._lib.icar_adv_batch_set_stream(self._b, C.c_void_p(cuda_stream)), self._b)
 

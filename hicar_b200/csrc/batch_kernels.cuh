@@ -127,19 +127,24 @@ __global__ void k_batch_prep(const BatchMember *__restrict__ mem, const int *__r
     }
 }
 
-// prefix over members of ceil(nx*nz*ny/256) blocks; every species of a cell in one thread
-__global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix, int nmem)
+// prefix over members of upwind_ngroups(S, sg) * ceil(nx*nz*ny/256) blocks:
+// each thread takes one species group of one cell
+__global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix, int nmem, int sg)
 {
     const int mi = find_owner(prefix, nmem, blockIdx.x);
     const BatchMember &m = mem[mi];
     const Geo g = m.g;
-    const size_t t = (size_t)(blockIdx.x - prefix[mi]) * blockDim.x + threadIdx.x;
+    const int grp = upwind_group(m.S, sg);
+    const int nblk = (int)(((size_t)g.nx * g.nz * g.ny + 255) / 256);
+    const int local = blockIdx.x - prefix[mi];
+    const int s0 = (local / nblk) * grp;
+    const size_t t = (size_t)(local % nblk) * blockDim.x + threadIdx.x;
     const int i = (int)(t % (size_t)g.nx);
     const size_t rest = t / (size_t)g.nx;
     const int k = (int)(rest % (size_t)g.nz);
     const int j = (int)(rest / (size_t)g.nz);
     if (j >= g.ny) return;
-    mp_upwind_at(g, i, k, j, m.q0, m.q1, m.out, m.S, m.Um, m.Vm, m.Wm, m.Gc, m.DJR);
+    mp_upwind_at(g, i, k, j, m.q0 + s0, m.q1 + s0, m.out + s0, min(grp, m.S - s0), m.Um, m.Vm, m.Wm, m.Gc, m.DJR);
 }
 
 // Persistent correction kernel: items are (member, species, i0, j0).

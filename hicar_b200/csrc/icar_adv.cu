@@ -68,6 +68,7 @@ struct icar_adv_domain {
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
     int path = 0;      // 0 = fused MPDATA kernel when eligible, 1 = staged kernels
     int mp_shape = 1;  // tile shape of the fused correction kernel (icar::mp_shape_ty)
+    int sp_group = 0;  // species per thread of the fused upwind pass (0 = all)
     // diagnostics: launch counter and optional event timing of the species kernels
     int64_t launches = 0;
     int64_t timed_launches = 0;
@@ -579,8 +580,9 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
     }
     const size_t nc = (size_t)g.nx * g.nz * g.ny;
     if (S > 0) {
-        icar::k_mp_upwind<<<blocks_for(nc, 256), 256, 0, h->stream>>>(g, sp, S, h->Um.p, h->Vm.p, h->Wm.p,
-                                                                      h->Gc.p, h->DJR.p);
+        const dim3 gu(blocks_for(nc, 256), icar::upwind_ngroups(S, h->sp_group));
+        icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, S, icar::upwind_group(S, h->sp_group), h->Um.p, h->Vm.p,
+                                                     h->Wm.p, h->Gc.p, h->DJR.p);
         icar::mp_corr_launch(h->stream, h->mp_shape, g, sp, S, h->opts.mpdata_fct, h->Um.p, h->Vm.p, h->Wp.p,
                              h->Gc.p, h->DJR.p, h->dz.p);
     }
@@ -970,6 +972,14 @@ int icar_adv_set_tile_shape(icar_adv_t *h, int32_t shape)
     return ICAR_ADV_OK;
 }
 
+int icar_adv_set_species_group(icar_adv_t *h, int32_t group)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (group < 0 || group > ICAR_ADV_MAX_SPECIES) return fail(h, ICAR_ADV_BAD_ARG, "species group %d out of range", group);
+    h->sp_group = group;
+    return ICAR_ADV_OK;
+}
+
 int icar_adv_tile_shapes(int32_t *n_shapes, int32_t *rows)
 {
     if (!n_shapes) return fail(nullptr, ICAR_ADV_BAD_ARG, "NULL argument");
@@ -1000,6 +1010,7 @@ struct icar_adv_batch {
     std::vector<icar_adv_t *> members;
     std::vector<double> dts;
     int shape = 1;
+    int sp_group = 0;  // species per thread of the upwind pass (0 = all)
     int fct = -1;
     bool tables_dirty = true, graph_dirty = true;
     int parity = 0;
@@ -1124,7 +1135,7 @@ int build_tables(icar_adv_batch_t *b)
         const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
         const size_t nc = (size_t)g.nx * g.nz * g.ny;
         prep[m + 1] = prep[m] + (int)((nf + 255) / 256);
-        up[m + 1] = up[m] + (h->desc.n_species > 0 ? (int)((nc + 255) / 256) : 0);
+        up[m + 1] = up[m] + icar::upwind_ngroups(h->desc.n_species, b->sp_group) * (int)((nc + 255) / 256);
         for (int s = 0; s < h->desc.n_species; s++) {
             if (h->forcing[s].p && h->nzone > 0) {
                 pairs.push_back(make_int2(m, s));
@@ -1217,7 +1228,7 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
         icar::k_batch_forcing<<<b->n_force, 256, 0, st>>>(mem, b->d_ints + b->off_f, b->d_pairs, b->n_pairs);
     if (b->n_prep > 0) icar::k_batch_prep<<<b->n_prep, 256, 0, st>>>(mem, b->d_ints, M);
     if (b->n_up > 0)
-        icar::k_batch_upwind<<<b->n_up, 256, 0, st>>>(mem, b->d_ints + b->off_up, M);
+        icar::k_batch_upwind<<<b->n_up, 256, 0, st>>>(mem, b->d_ints + b->off_up, M, b->sp_group);
     cudaMemsetAsync(b->d_ints + b->off_counter, 0, sizeof(int), st);
     if (b->n_items > 0)
         icar::batch_corr_launch(st, b->shape, b->ctas, b->fct, mem, b->d_items, b->n_items,
@@ -1338,6 +1349,17 @@ int icar_adv_batch_set_tile_shape(icar_adv_batch_t *b, int32_t shape)
     if (shape < 0 || shape >= icar::MP_NSHAPES) return bfail(b, ICAR_ADV_BAD_ARG, "tile shape out of range");
     if (shape != b->shape) {
         b->shape = shape;
+        b->tables_dirty = b->graph_dirty = true;
+    }
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_set_species_group(icar_adv_batch_t *b, int32_t group)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    if (group < 0 || group > ICAR_ADV_MAX_SPECIES) return bfail(b, ICAR_ADV_BAD_ARG, "species group out of range");
+    if (group != b->sp_group) {
+        b->sp_group = group;
         b->tables_dirty = b->graph_dirty = true;
     }
     return ICAR_ADV_OK;
@@ -1575,7 +1597,7 @@ extern "C" int icar_adv_advect_noalloc(const icar_adv_noalloc_args *a)
         sp.q0[0] = a->q_in[s];
         sp.q1[0] = q1;
         sp.out[0] = a->q_out[s];
-        icar::k_mp_upwind<<<blocks_for(ncell, 256), 256, 0, st>>>(g, sp, 1, Um, Vm, Wm, Gc, DJR);
+        icar::k_mp_upwind<<<blocks_for(ncell, 256), 256, 0, st>>>(g, sp, 1, 1, Um, Vm, Wm, Gc, DJR);
         icar::mp_corr_launch(st, 1, g, sp, 1, a->mpdata_fct ? 1 : 0, Um, Vm, Wp, Gc, DJR, a->advection_dz);
     }
     ce = cudaGetLastError();

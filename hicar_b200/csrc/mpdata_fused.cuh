@@ -135,8 +135,11 @@ __device__ __forceinline__ void mp_upwind_at(const Geo &g, int i, int k, int j, 
     }
 }
 
-__global__ void k_mp_upwind(Geo g, SpeciesPtrs sp, int S, const float *__restrict__ U, const float *__restrict__ V,
-                            const float *__restrict__ W, const float *__restrict__ Gc, const float *__restrict__ DJR)
+// Species group: blockIdx.y takes species [y*sg, min(S, (y+1)*sg)) of every
+// cell, so a small domain can trade the reuse of its winds for more blocks.
+__global__ void k_mp_upwind(Geo g, const __grid_constant__ SpeciesPtrs sp, int S, int sg,
+                            const float *__restrict__ U, const float *__restrict__ V, const float *__restrict__ W,
+                            const float *__restrict__ Gc, const float *__restrict__ DJR)
 {
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int i = (int)(t % (size_t)g.nx);
@@ -144,7 +147,16 @@ __global__ void k_mp_upwind(Geo g, SpeciesPtrs sp, int S, const float *__restric
     const int k = (int)(rest % (size_t)g.nz);
     const int j = (int)(rest / (size_t)g.nz);
     if (j >= g.ny) return;
-    mp_upwind_at(g, i, k, j, sp.q0, sp.q1, sp.out, S, U, V, W, Gc, DJR);
+    const int s0 = blockIdx.y * sg;
+    mp_upwind_at(g, i, k, j, sp.q0 + s0, sp.q1 + s0, sp.out + s0, min(sg, S - s0), U, V, W, Gc, DJR);
+}
+
+// Blocks of the species dimension for a species group (0 = all species).
+__host__ __device__ inline int upwind_group(int S, int sg) { return sg <= 0 || sg > S ? S : sg; }
+__host__ __device__ inline int upwind_ngroups(int S, int sg)
+{
+    const int g = upwind_group(S, sg);
+    return g > 0 ? (S + g - 1) / g : 0;
 }
 
 namespace mpf {

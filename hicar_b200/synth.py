@@ -308,13 +308,16 @@ def periodic_y_case(ny: int = 100, nx: int = 3, nz: int = 3, cfl: float = 0.25, 
 
 # ------------------------------------------------- on-device generation
 def device_member(nx: int, ny: int, nz: int, seed: int, device: int = 0, dx: float = 4000.0,
-                  dz: float = 500.0, species=ALL12):
+                  dz: float = 500.0, species=ALL12, terrain_kind: str = "ridge", U: float | None = None,
+                  noise: float = 0.02, dt: float = 20.0, rms: float = 800.0, hmax: float = 4000.0):
     """A config-1-style domain generated directly in GPU memory with torch
-    (for served requests, whose inputs must appear in milliseconds): Gaussian
-    ridge, Gal-Chen jacobians, uniform westerly with seeded noise, w from
-    discrete continuity, qv/theta profiles and clustered lognormal
-    hydrometeors with ~70 % zeros.  Returns (dict of float32 CUDA tensors in
-    the Fortran layout of Case, dt)."""
+    (for served requests, whose inputs must appear in milliseconds, and for
+    domains too large to build on the host): a Gaussian ridge (terrain_kind=
+    "ridge") or random-phase power-law terrain of the given RMS clipped at
+    hmax (terrain_kind="fractal"), Gal-Chen jacobians, uniform westerly (U, or a
+    seeded 8..12 m/s) with seeded relative noise, w from discrete continuity,
+    qv/theta profiles and clustered lognormal hydrometeors with ~70 % zeros.
+    Returns (dict of float32 CUDA tensors in the Fortran layout of Case, dt)."""
     import torch
     g = torch.Generator(device=f"cuda:{device}")
     g.manual_seed(int(seed))
@@ -325,8 +328,22 @@ def device_member(nx: int, ny: int, nz: int, seed: int, device: int = 0, dx: flo
     x = (torch.arange(nx, device=dev, dtype=f32) - (nx - 1) / 2.0) * dx
     y = (torch.arange(ny, device=dev, dtype=f32) - (ny - 1) / 2.0) * dx
     h = float(800.0 + 1200.0 * r(1).item())
-    terrain = h * torch.exp(-(x[None, :] ** 2 + y[:, None] ** 2) / 20000.0 ** 2)
+    if terrain_kind == "fractal":
+        kx = torch.fft.rfftfreq(nx, d=dx, device=dev)
+        ky = torch.fft.fftfreq(ny, d=dx, device=dev)
+        kk = torch.sqrt(kx[None, :] ** 2 + ky[:, None] ** 2)
+        kk[0, 0] = float("inf")
+        phase = 2 * torch.pi * torch.rand(kk.shape, generator=g, device=dev, dtype=torch.float64)
+        spec = torch.polar(kk.double() ** -1.5, phase)
+        t = torch.fft.irfft2(spec, s=(ny, nx))
+        t = (t - t.mean()) / (t.std() + 1e-30) * rms
+        terrain = torch.clamp(t - t.min(), max=hmax).to(f32)
+        del kk, phase, spec, t
+    else:
+        terrain = h * torch.exp(-(x[None, :] ** 2 + y[:, None] ** 2) / 20000.0 ** 2)
     H = dz * nz
+    if float(terrain.max()) >= H:
+        raise ValueError("terrain reaches the model lid")
     jac1 = (H - terrain) / H
     jac = jac1[:, None, :].expand(ny, nz, nx).contiguous()
     dzi = dz * jac
@@ -342,9 +359,9 @@ def device_member(nx: int, ny: int, nz: int, seed: int, device: int = 0, dx: flo
     jw[:, nz - 1] = jac[:, nz - 1]
     jw[:, :nz - 1] = (dzi[:, :-1] * jac[:, :-1] + dzi[:, 1:] * jac[:, 1:]) / (dzi[:, :-1] + dzi[:, 1:])
     adz = torch.full((ny, nz, nx), dz, device=dev, dtype=f32)
-    U = float(8.0 + 4.0 * r(1).item())
-    u = U + 0.02 * U * n(ny, nz, nx + 1)
-    v = 0.02 * U * n(ny + 1, nz, nx)
+    U = float(8.0 + 4.0 * r(1).item()) if U is None else float(U)
+    u = U + noise * U * n(ny, nz, nx + 1)
+    v = noise * U * n(ny + 1, nz, nx)
     div = ((u * ju)[:, :, 1:] - (u * ju)[:, :, :-1] + (v * jv)[1:] - (v * jv)[:-1]) / dx
     w = torch.empty(ny, nz, nx, device=dev, dtype=f32)
     w[:, 0] = (0 - div[:, 0] * adz[:, 0]) / jw[:, 0]
@@ -381,4 +398,12 @@ def device_member(nx: int, ny: int, nz: int, seed: int, device: int = 0, dx: flo
     for k in list(out):
         if k != "species":
             out[k] = out[k].to(f32).contiguous()
-    return out, 20.0
+    return out, float(dt)
+
+
+def device_config5(seed: int = 0, nx: int = 2048, ny: int = 2048, nz: int = 60, device: int = 0):
+    """The large single domain (2048x2048x60, dx 250 m, fractal terrain up to
+    4000 m, 12 fields, dt 1 s) generated on the device: building it on the
+    host would take minutes and tens of GB of host memory."""
+    return device_member(nx, ny, nz, seed, device=device, dx=250.0, dz=350.0, terrain_kind="fractal", U=15.0,
+                         noise=0.05, dt=1.0, rms=800.0, hmax=4000.0)

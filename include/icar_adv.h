@@ -219,6 +219,7 @@ int icar_adv_batch_add(icar_adv_batch_t *b, icar_adv_t *member, double dt_second
 int icar_adv_batch_remove(icar_adv_batch_t *b, icar_adv_t *member);
 int icar_adv_batch_set_dt(icar_adv_batch_t *b, icar_adv_t *member, double dt_seconds);
 int icar_adv_batch_set_tile_shape(icar_adv_batch_t *b, int32_t shape);
+int icar_adv_batch_set_species_group(icar_adv_batch_t *b, int32_t group);
 int icar_adv_batch_step(icar_adv_batch_t *b);
 int icar_adv_batch_sync(icar_adv_batch_t *b);
 int icar_adv_batch_set_stream(icar_adv_batch_t *b, void *cuda_stream);
@@ -277,10 +278,15 @@ typedef struct {
 
 int icar_adv_advect_noalloc(const icar_adv_noalloc_args *args);
 
-/* Tile shape of the fused MPDATA kernel (no reference counterpart; chosen per
- * grid shape by the autotuner).  icar_adv_tile_shapes reports how many shapes
- * exist and the output rows per tile of each (rows may be NULL). */
+/* Launch shape of the fused MPDATA kernels (no reference counterpart; chosen
+ * per grid shape by the autotuner, hicar_b200/autotune.py).  The tile shape
+ * selects the output rows per tile of the correction kernel;
+ * icar_adv_tile_shapes reports how many shapes exist and the rows of each
+ * (rows may be NULL).  The species group is the number of species one thread
+ * of the donor-cell pass takes (0 = all, the default; 1..32).  Neither
+ * changes any result. */
 int icar_adv_set_tile_shape(icar_adv_t *h, int32_t shape);
+int icar_adv_set_species_group(icar_adv_t *h, int32_t group);
 int icar_adv_tile_shapes(int32_t *n_shapes, int32_t *rows);
 
 /* Kernel selection for testing: 0 = fused MPDATA kernel where it applies
