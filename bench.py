@@ -191,21 +191,16 @@ def run_reference(args):
 # --------------------------------------------------------------- GPU arm
 def run_b200(args):
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-
-    from hicar_b200 import _lib as L
+    from hicar_b200 import _lib as L, replicas as R
     from hicar_b200.advection import Domain, Options, adv_init
 
+    rk = R.from_env()
+    world, rank, local = rk.world, rk.rank, rk.local
+    torch.cuda.set_device(local)
+    R.init(rk, "nccl")
     lib = L.load()
-    case, desc = make_case(args.workload, 100 + rank)
+    case, desc = make_case(args.workload, R.replica_seed(100, rk))
     S = len(case.species)
     cells = case.cells()
     opts = Options()
@@ -227,8 +222,7 @@ def run_b200(args):
         L.check(lib.icar_adv_step(h, C.c_double(case.dt), 0), h)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        R.barrier(rk)
 
     for _ in range(args.warmup):
         step()
@@ -252,16 +246,20 @@ def run_b200(args):
     clk = clocks.stop()
     kms, klaunch, alll, passes = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
     L.check(lib.icar_adv_profile_read(h, C.byref(kms), C.byref(klaunch), C.byref(alll), C.byref(passes)), h)
+    cms, claunch = C.c_double(), C.c_int64()
+    L.check(lib.icar_adv_profile_read_correction(h, C.byref(cms), C.byref(claunch)), h)
     L.check(lib.icar_adv_profile(h, 0), h)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = cells * S * args.steps * world / (ms_max / 1e3)
+    ms_max = R.max_over_ranks(rk, ms)
+    value = R.whole_job_rate(cells * S * args.steps, world, ms_max / 1e3)
 
     # ---- roofline of the species kernels ------------------------------
     from hicar_b200 import roofline
-    rl = roofline.species_pass(case.nx, case.ny, case.nz, S, kms.value, passes.value)
+    step_rl = roofline.species_pass(case.nx, case.ny, case.nz, S, kms.value, passes.value)
+    if claunch.value > 0:
+        rl = roofline.correction_kernel(case.nx, case.ny, case.nz, S, cms.value, claunch.value)
+        rl["advect_call"] = step_rl
+    else:                                       # staged path: the whole advect call
+        rl = step_rl
 
     # ---- end to end through the C ABI with pinned host buffers ---------
     if args.quick:
@@ -269,8 +267,7 @@ def run_b200(args):
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "quick": True,
                               "ms_per_step": ms_max / args.steps, "roofline": rl}), flush=True)
         d.close()
-        if world > 1:
-            dist.destroy_process_group()
+        R.finalize(rk)
         return
     host = {k: torch.from_numpy(v.copy()).pin_memory() for k, v in case.species.items()}
     ids = {k: L.SPECIES_IDS[k] for k in case.species}
@@ -290,11 +287,8 @@ def run_b200(args):
     for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_val = cells * S * e2e_steps * world / float(t.item())
+    e2e_s = R.max_over_ranks(rk, time.perf_counter() - t0)
+    e2e_val = R.whole_job_rate(cells * S * e2e_steps, world, e2e_s)
     bytes_io = cells * S * 4
 
     cpu = None
@@ -325,8 +319,7 @@ def run_b200(args):
         }
         print(json.dumps(out), flush=True)
     d.close()
-    if world > 1:
-        dist.destroy_process_group()
+    R.finalize(rk)
 
 
 def set_launch_shape(d, args) -> dict:
@@ -350,11 +343,13 @@ def run_large(args):
     shape against the autotuned one (every tile shape and species group timed
     on this domain itself; the state advances while they are timed)."""
     import torch
-    from hicar_b200 import _lib as L, autotune, roofline, synth
+    from hicar_b200 import _lib as L, autotune, replicas as R, roofline, synth
     from hicar_b200.advection import Domain, Options, advect
 
+    if not R.from_env().is_root:
+        return                                   # a single domain on one GPU: the other ranks have no work
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
+    rank = 0
     torch.cuda.set_device(local)
     nx, ny, nz = 2048, 2048, 60
     fields, dt = synth.device_config5(seed=3, nx=nx, ny=ny, nz=nz, device=local)
@@ -385,13 +380,15 @@ def run_large(args):
         torch.cuda.synchronize()
         kms, kl, al, ps = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
         L.check(lib.icar_adv_profile_read(h, C.byref(kms), C.byref(kl), C.byref(al), C.byref(ps)), h)
+        cms, cl = C.c_double(), C.c_int64()
+        L.check(lib.icar_adv_profile_read_correction(h, C.byref(cms), C.byref(cl)), h)
         L.check(lib.icar_adv_profile(h, 0), h)
-        return e0.elapsed_time(e1), kms.value, ps.value, al.value
+        return e0.elapsed_time(e1), (kms.value, ps.value, cms.value, cl.value), al.value
 
     d.set_launch_shape(1, 0)
     for _ in range(args.warmup):
         step()
-    ms_plain, _, _, _ = timed(args.steps)
+    ms_plain, _, _ = timed(args.steps)
     measured = {}
     for shape in range(len(autotune.TILE_ROWS)):
         for group in autotune.species_groups(S):
@@ -405,9 +402,10 @@ def run_large(args):
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.4)
-    ms, kms, passes, launches = timed(args.steps)
+    ms, (kms, passes, cms, cl), launches = timed(args.steps)
     clk = clocks.stop()
-    rl = roofline.species_pass(nx, ny, nz, S, kms, passes)
+    rl = roofline.correction_kernel(nx, ny, nz, S, cms, cl)
+    rl["advect_call"] = roofline.species_pass(nx, ny, nz, S, kms, passes)
     if rank == 0:
         print(json.dumps({
             "metric": METRIC, "value": cs * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
@@ -453,20 +451,15 @@ def make_ensemble(n: int, seed: int):
 def run_ensemble(args):
     import torch
 
-    from hicar_b200 import _lib as L, roofline
+    from hicar_b200 import _lib as L, replicas as R, roofline
     from hicar_b200.advection import Domain, Options, adv_init
     from hicar_b200.batch import Batch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    cases = make_ensemble(args.members, 7 + rank)
+    rk = R.from_env()
+    world, rank, local = rk.world, rk.rank, rk.local
+    cases = make_ensemble(args.members, R.replica_seed(7, rk))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    R.init(rk, "nccl", timeout_s=600)
     lib = L.load()
     opts = Options()
     stream = torch.cuda.Stream()
@@ -482,8 +475,7 @@ def run_ensemble(args):
     cs_step = sum(c.cells() * len(c.species) for c in cases)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        R.barrier(rk)
 
     def timed(fn, steps):
         barrier()
@@ -495,12 +487,7 @@ def run_ensemble(args):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return R.max_over_ranks(rk, e0.elapsed_time(e1))
 
     # ---- plain: one domain per launch sequence, members one after another
     def plain_step():
@@ -511,7 +498,7 @@ def run_ensemble(args):
         plain_step()
     plain_steps = max(3, args.steps // 4)
     plain_ms = timed(plain_step, plain_steps)
-    plain_value = cs_step * plain_steps * world / (plain_ms / 1e3)
+    plain_value = R.whole_job_rate(cs_step * plain_steps, world, plain_ms / 1e3)
 
     # ---- batched: every member in one graph launch per step
     b = Batch(device=local)
@@ -534,7 +521,7 @@ def run_ensemble(args):
     clk = clocks.stop()
     prof = b.profile_read()
     b.profile(False)
-    value = cs_step * args.steps * world / (ms / 1e3)
+    value = R.whole_job_rate(cs_step * args.steps, world, ms / 1e3)
     bytes_step = sum(c.cells() * (8 * len(c.species) + 32) for c in cases)
     peak, kind = roofline.hbm_peak()
     step_ms = prof["ms"] / max(prof["steps"], 1)
@@ -549,6 +536,7 @@ def run_ensemble(args):
         b.close()
         for d in doms:
             d.close()
+        R.finalize(rk)
         return
 
     # ---- end to end: host buffers in and out of every member every step
@@ -571,12 +559,8 @@ def run_ensemble(args):
     for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_val = cs_step * e2e_steps * world / e2e_s
+    e2e_s = R.max_over_ranks(rk, time.perf_counter() - t0)
+    e2e_val = R.whole_job_rate(cs_step * e2e_steps, world, e2e_s)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -611,8 +595,7 @@ def run_ensemble(args):
     b.close()
     for d in doms:
         d.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    R.finalize(rk)
 
 
 # -------------------------------------------------------------- served
@@ -622,8 +605,11 @@ def run_served(args):
     counts are scaled by --serve-duration and --serve-steps-scale so a run
     fits in minutes)."""
     import torch
+    from hicar_b200 import replicas as R
     from hicar_b200.serve import Server, poisson_requests
 
+    if not R.from_env().is_root:
+        return                                   # one server on one GPU: the other ranks have no work
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     smin, smax = int(round(50 * args.serve_steps_scale)), int(round(500 * args.serve_steps_scale))

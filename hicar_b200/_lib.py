@@ -95,6 +95,7 @@ _PROTOS = {
     "icar_adv_last_error": (C.c_char_p, [C.c_void_p]),
     "icar_adv_set_path": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "icar_adv_profile_read_correction": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
     "icar_adv_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_set_species_group": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),

@@ -74,6 +74,7 @@ struct icar_adv_domain {
     int64_t timed_launches = 0;
     bool profiling = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> corr_events;  // the fused correction kernel alone
     icar_adv_batch *batch = nullptr;  // batch this domain is a member of, if any
     std::string err;
 };
@@ -583,8 +584,18 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
         const dim3 gu(blocks_for(nc, 256), icar::upwind_ngroups(S, h->sp_group));
         icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, S, icar::upwind_group(S, h->sp_group), h->Um.p, h->Vm.p,
                                                      h->Wm.p, h->Gc.p, h->DJR.p);
+        cudaEvent_t c0 = nullptr, c1 = nullptr;
+        if (h->profiling) {
+            cudaEventCreate(&c0);
+            cudaEventCreate(&c1);
+            cudaEventRecord(c0, h->stream);
+        }
         icar::mp_corr_launch(h->stream, h->mp_shape, g, sp, S, h->opts.mpdata_fct, h->Um.p, h->Vm.p, h->Wp.p,
                              h->Gc.p, h->DJR.p, h->dz.p);
+        if (h->profiling) {
+            cudaEventRecord(c1, h->stream);
+            h->corr_events.emplace_back(c0, c1);
+        }
     }
     e = check_launch(h, "fused MPDATA kernels", S > 0 ? 3 : 1);
     if (e) return e;
@@ -791,10 +802,11 @@ int icar_adv_destroy(icar_adv_t *h)
     for (auto &b : h->q) release(b);
     for (auto &b : h->qn) release(b);
     for (auto &b : h->q1s) release(b);
-    for (auto &p : h->events) {
-        cudaEventDestroy(p.first);
-        cudaEventDestroy(p.second);
-    }
+    for (auto *v : {&h->events, &h->corr_events})
+        for (auto &p : *v) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
     for (auto &b : h->forcing) release(b);
     for (auto &b : h->dqdt) release(b);
     if (h->filter_dev) cudaFree(h->filter_dev);
@@ -934,11 +946,13 @@ int icar_adv_profile(icar_adv_t *h, int32_t enable)
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
     cudaSetDevice(h->desc.device);
     cudaStreamSynchronize(h->stream);
-    for (auto &p : h->events) {
-        cudaEventDestroy(p.first);
-        cudaEventDestroy(p.second);
+    for (auto *v : {&h->events, &h->corr_events}) {
+        for (auto &p : *v) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+        v->clear();
     }
-    h->events.clear();
     h->profiling = enable != 0;
     h->launches = 0;
     h->timed_launches = 0;
@@ -961,6 +975,22 @@ int icar_adv_profile_read(icar_adv_t *h, double *species_kernel_ms, int64_t *spe
     if (species_kernel_launches) *species_kernel_launches = h->timed_launches;
     if (all_launches) *all_launches = h->launches;
     if (species_passes) *species_passes = (int64_t)h->events.size();
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_profile_read_correction(icar_adv_t *h, double *ms, int64_t *launches)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    double total = 0.0;
+    for (auto &p : h->corr_events) {
+        float t = 0.0f;
+        CUDA_TRY(h, cudaEventElapsedTime(&t, p.first, p.second));
+        total += t;
+    }
+    if (ms) *ms = total;
+    if (launches) *launches = (int64_t)h->corr_events.size();
     return ICAR_ADV_OK;
 }
 

@@ -7,6 +7,12 @@ once per step (32 B per cell), shared by the S species:
     8 + 32/S bytes per cell-species  (10.67 B at S=12, 40 B at S=1).
 One advect call (all S species) therefore moves cells * (8*S + 32)
 algorithmic bytes.  advection_dz is one value per level and is not counted.
+
+The dominant kernel of the step, the fused correction kernel (k_mp_corr),
+reads q0 and q1 and writes the new state of every species (12 B per
+cell-species) and reads six species-independent fields once (U_m, V_m,
+W_m/dz, J*rho, dz*J*rho and dz: 24 B per cell):
+    12 + 24/S bytes per cell-species  (14 B at S=12).
 """
 from __future__ import annotations
 
@@ -44,4 +50,31 @@ def species_pass(nx: int, ny: int, nz: int, S: int, total_ms: float, passes: int
         "peak_kind": kind, "algorithmic_bytes_per_launch": per_pass,
         "launch_ms": (total_ms / passes) if passes else None,
         "bytes_model": "8 + 32/S B per cell-species; one launch = the kernels of one advect call",
+    }
+
+
+# DRAM bytes (read + write) per cell-species of one k_mp_corr launch, from
+# the ncu capture summarised in profiles/k_mp_corr_256x256x40x12.md
+# (256x256x40, 12 species, tile shape 16 rows, FCT on).
+CORR_DRAM_BYTES_PER_CS = 14.03
+
+
+def correction_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launches: int) -> dict:
+    """Roofline entry for the fused correction kernel alone, timed with CUDA
+    events around its launches on the launching stream."""
+    peak, kind = hbm_peak()
+    cells = nx * ny * nz
+    per_launch = cells * (12.0 * S + 24.0)
+    achieved = per_launch / (total_ms / launches / 1e3) / 1e9 if launches > 0 and total_ms > 0 else None
+    traffic = cells * S * CORR_DRAM_BYTES_PER_CS if CORR_DRAM_BYTES_PER_CS else None
+    return {
+        "kernel": "k_mp_corr (pseudo-velocities + FCT + corrective pass, all species)",
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+        "peak_kind": kind, "algorithmic_bytes_per_launch": per_launch,
+        "launch_ms": (total_ms / launches) if launches else None,
+        "bytes_model": "12 + 24/S B per cell-species; one launch = all species of one advect call",
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per cell-species of a "
+                           "256x256x40x12 launch, scaled to this launch by cell-species")
+        if CORR_DRAM_BYTES_PER_CS else None,
     }

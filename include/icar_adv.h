@@ -199,6 +199,9 @@ const char *icar_adv_last_error(const icar_adv_t *h);
 int icar_adv_profile(icar_adv_t *h, int32_t enable);
 int icar_adv_profile_read(icar_adv_t *h, double *species_kernel_ms, int64_t *species_kernel_launches,
                           int64_t *all_launches, int64_t *species_passes);
+/* Summed device time and launch count of the fused correction kernel alone
+ * (the dominant kernel of the fused MPDATA step) since icar_adv_profile(h, 1). */
+int icar_adv_profile_read_correction(icar_adv_t *h, double *ms, int64_t *launches);
 
 /* ---------------------------------------------------------------------------
  * Batched form (no reference counterpart: the reference advances one domain
