@@ -203,3 +203,25 @@ def test_fused_and_staged_agree_over_many_steps(oracle_lib):
     b = gpu_run(case, Options(), 40, staged=True)
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("scale", [1e-28, 1e-36, 1e30, 1.0])
+def test_fused_exact_at_extreme_magnitudes(oracle_lib, scale):
+    """Fields scaled to the edges of the FP32 range: subnormal values and
+    quotients (1e-28, 1e-36), values near the overflow threshold (1e30),
+    and tiny values (below 1e-33) mixed into ordinary ones.  The fused
+    kernel still equals the oracle cell for cell."""
+    O = oracle_lib
+    case = synth.config2(seed=44, nx=61, ny=47, nz=9)
+    case.species = {k: case.species[k] for k in ("qv", "qc", "nr", "theta")}
+    rng = np.random.default_rng(3)
+    for k, q in case.species.items():
+        if scale == 1.0:
+            tiny = rng.random(q.shape) < 0.3
+            case.species[k] = np.where(tiny, np.float32(1e-33) * rng.random(q.shape).astype(np.float32), q)
+        else:
+            case.species[k] = (q * np.float32(scale)).astype(np.float32)
+    for fct in (1, 0):
+        o = O.make_opts(mpdata_fct=fct)
+        ref = O.run_steps(case, o, case.dt, 3)
+        assert_exact(gpu_run(case, options_from(o), 3), ref, label=f"scale={scale} fct={fct} ")
