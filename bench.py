@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="full_species",
-                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large"])
+                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large", "wind"])
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-duration", type=float, default=6.0)
     p.add_argument("--serve-steps-scale", type=float, default=0.1)
@@ -427,6 +427,75 @@ def run_large(args):
     d.close()
 
 
+# ------------------------------------------------------------ wind balance
+def run_wind(args):
+    """balance_uvw and compute_dt (the per-step wind operations beside
+    advection) on the full-species domain, each timed with CUDA events on
+    the library's stream, against the HBM roofline of their bytes."""
+    import torch
+    from hicar_b200 import _lib as L, replicas as R, roofline
+    from hicar_b200.advection import Domain, Options, Parameters, adv_init, balance_uvw
+
+    if not R.from_env().is_root:
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    case, desc = make_case("full_species", 100)
+    opts = Options(parameters=Parameters(advect_density=True))
+    d = Domain.from_case(case, device=local)
+    adv_init(d, opts)
+    lib = L.load()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
+    dz = np.ascontiguousarray(case.dz_levels, np.float32)
+    dzp = dz.ctypes.data_as(C.POINTER(C.c_float))
+    out = C.c_float()
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def dt_device_only():
+        # the maxima kernel alone: icar_adv_compute_dt also copies 16 bytes back and waits
+        L.check(lib.icar_adv_compute_dt(d.handle, dzp, C.c_float(0.9), 3, 0, C.byref(out)), d.handle)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    ms_bal = timed(lambda: balance_uvw(d, opts), args.steps)
+    t0 = time.perf_counter()
+    for _ in range(20):
+        dt_device_only()
+    ms_dt_host = (time.perf_counter() - t0) / 20 * 1e3
+    clk = clocks.stop()
+    cells = case.cells()
+    peak, kind = roofline.hbm_peak()
+    bal_bytes = cells * 32.0                 # u, v, J_u, J_v, rho, dz, J_w read, w written (4 B each)
+    dt_bytes = cells * 12.0                  # u, v, w read
+    d.close()
+    print(json.dumps({
+        "metric": "wind balance cells/s", "value": cells / (ms_bal / 1e3), "unit": "cells/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_bal, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "balance_uvw (advect_density) and compute_dt on the " + desc},
+        "roofline": {"kernel": "k_balance_uvw", "bound": "hbm", "achieved": bal_bytes / (ms_bal / 1e3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": bal_bytes / (ms_bal / 1e3) / 1e9 / peak,
+                     "traffic": None, "peak_kind": kind, "algorithmic_bytes_per_launch": bal_bytes,
+                     "bytes_model": "32 B per cell: seven input fields read and w written once"},
+        "compute_dt": {"ms_per_call_host_synchronous": ms_dt_host, "algorithmic_bytes": dt_bytes,
+                       "dt_seconds": out.value},
+        "clocks": clk}), flush=True)
+
+
 # ------------------------------------------------------------ ensemble
 ENSEMBLE_DESC = ("batched uneven ensemble: 64 independent domains, nx,ny ~ U[64,384], nz ~ U[20,50], "
                  "12 fields each, dt 20 s, one graph launch per step vs 64 plain launches")
@@ -648,6 +717,8 @@ def main():
         run_served(args)
     elif args.workload == "large":
         run_large(args)
+    elif args.workload == "wind":
+        run_wind(args)
     else:
         run_b200(args)
 

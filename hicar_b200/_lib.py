@@ -96,6 +96,9 @@ _PROTOS = {
     "icar_adv_set_path": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_profile_read_correction": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+    "icar_adv_balance_uvw": (C.c_int, [C.c_void_p]),
+    "icar_adv_compute_dt": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32,
+                                      C.POINTER(C.c_float)]),
     "icar_adv_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_set_species_group": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),

@@ -49,6 +49,8 @@ class PhysicsOptions:
 @dataclass
 class TimeOptions:
     RK3: bool = False
+    cfl_reduction_factor: float = 0.9   # time_options defaults, options_obj.f90 (time_parameters namelist)
+    cfl_strictness: int = 3
 
 
 @dataclass
@@ -312,6 +314,31 @@ def advect(domain: Domain, options: Options, dt: float) -> None:
     device; fetch() or sync() to wait)."""
     domain._flush()
     L.check(L.load().icar_adv_advect(domain.handle, C.c_float(dt)), domain.handle)
+
+
+def balance_uvw(domain: Domain, options: Options) -> None:
+    """wind.f90:88-164: rebuild the resident w from the horizontal
+    divergence of u and v (density weighted with advect_density, the setting
+    the handle was created with).  Asynchronous; fetch("w") to read it."""
+    domain._flush()
+    L.check(L.load().icar_adv_balance_uvw(domain.handle), domain.handle)
+
+
+def compute_dt(domain: Domain, options: Options, dz_levels, use_density: bool = False) -> float:
+    """time_step.f90:51-168: the largest stable time step (seconds) for the
+    resident winds, options.time_options.cfl_reduction_factor and
+    cfl_strictness, and the 1-D dz_levels.  Raises IcarAdvError
+    (CFL_VIOLATION) when it is below 0.1 s, where the reference stops."""
+    domain._flush()
+    dz = np.ascontiguousarray(dz_levels, np.float32)
+    if dz.size != domain.nz:
+        raise ValueError("dz_levels must have nz entries")
+    out = C.c_float()
+    t = options.time_options
+    L.check(L.load().icar_adv_compute_dt(domain.handle, dz.ctypes.data_as(C.POINTER(C.c_float)),
+                                         C.c_float(t.cfl_reduction_factor), int(t.cfl_strictness),
+                                         int(bool(use_density)), C.byref(out)), domain.handle)
+    return float(out.value)
 
 
 def step(domain: Domain, options: Options, dt_seconds: float, enforce_limits: bool = False) -> None:

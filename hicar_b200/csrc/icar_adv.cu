@@ -23,6 +23,7 @@
 #include "mpdata_kernels.cuh"
 #include "std_kernels.cuh"
 #include "batch_kernels.cuh"
+#include "wind_kernels.cuh"
 
 using icar::Geo;
 
@@ -63,6 +64,7 @@ struct icar_adv_domain {
     DevBuf Um, Vm, Wm;
     DevBuf q1, u2, v2, w2, u2l, v2l, w2l;      // MPDATA staged scratch
     DevBuf Gc, DJR, Wp;                        // fused path: J*rho, dz*J*rho, W_m/dz
+    DevBuf dtbuf;                              // compute_dt: 4 maxima then dz_levels (nz)
     std::vector<DevBuf> qn, q1s;               // fused path: next state and pass-1 result per species
     bool fused_ready = false;
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
@@ -797,7 +799,7 @@ int icar_adv_destroy(icar_adv_t *h)
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
                       &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
                       &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp, &h->Gc,
-                      &h->DJR, &h->Wp})
+                      &h->DJR, &h->Wp, &h->dtbuf})
         release(*b);
     for (auto &b : h->q) release(b);
     for (auto &b : h->qn) release(b);
@@ -900,6 +902,60 @@ int icar_adv_enforce_limits(icar_adv_t *h)
     for (int s = 0; s < h->desc.n_species; s++)
         icar::k_enforce_limits<<<blocks_for(h->n_cell, 256), 256, 0, h->stream>>>(h->g, h->q[s].p);
     return check_launch(h, "enforce_limits", h->desc.n_species);
+}
+
+int icar_adv_balance_uvw(icar_adv_t *h)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (h->batch) return fail(h, ICAR_ADV_BAD_ARG, "domain is a batch member");
+    cudaSetDevice(h->desc.device);
+    const char *missing = nullptr;
+    const int adv_den = h->opts.advect_density;
+    if (!h->have_u) missing = "u";
+    else if (!h->have_v) missing = "v";
+    else if (!h->have_jac_u) missing = "jacobian_u";
+    else if (!h->have_jac_v) missing = "jacobian_v";
+    else if (!h->have_jac_w) missing = "jacobian_w";
+    else if (!h->have_dz) missing = "advection_dz";
+    else if (adv_den && !h->have_rho) missing = "density";
+    if (missing) return fail(h, ICAR_ADV_NOT_READY, "field %s was never set", missing);
+    const Geo &g = h->g;
+    const float *rho = adv_den ? h->rho.p : h->jac.p;  // only read when advect_density
+    icar::k_balance_uvw<<<blocks_for((size_t)g.nx * g.ny, 128), 128, 0, h->stream>>>(
+        g, h->hs, h->desc.dx, adv_den, h->u.p, h->v.p, rho, h->dz.p, h->jac_u.p, h->jac_v.p, h->jac_w.p, h->w.p);
+    h->have_w = true;
+    return check_launch(h, "balance_uvw");
+}
+
+int icar_adv_compute_dt(icar_adv_t *h, const float *dz_levels, float cfl, int32_t cfl_strictness,
+                        int32_t use_density, float *dt)
+{
+    if (!h || !dz_levels || !dt) return fail(h, ICAR_ADV_BAD_ARG, "NULL argument");
+    if (cfl_strictness < 1 || cfl_strictness > 5) return fail(h, ICAR_ADV_BAD_ARG, "cfl_strictness must be 1..5");
+    cudaSetDevice(h->desc.device);
+    if (!h->have_u || !h->have_v || !h->have_w) return fail(h, ICAR_ADV_NOT_READY, "u, v and w must be set");
+    const Geo &g = h->g;
+    int e = alloc(h, h->dtbuf, 4 + (size_t)g.nz);
+    if (e) return e;
+    unsigned *d_out = reinterpret_cast<unsigned *>(h->dtbuf.p);
+    float *d_dz = h->dtbuf.p + 4;
+    CUDA_TRY(h, cudaMemcpyAsync(d_dz, dz_levels, sizeof(float) * g.nz, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaMemsetAsync(d_out, 0, 4 * sizeof(unsigned), h->stream));
+    const size_t total = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+    const unsigned blocks = (unsigned)std::min<size_t>(blocks_for(total, 256), 148 * 8);
+    icar::k_dt_maxima<<<blocks, 256, 0, h->stream>>>(g, h->hs, h->desc.dx, h->u.p, h->v.p, h->w.p, d_dz, d_out);
+    e = check_launch(h, "compute_dt");
+    if (e) return e;
+    unsigned bits[4];
+    CUDA_TRY(h, cudaMemcpyAsync(bits, d_out, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    float m[4];
+    memcpy(m, bits, sizeof(m));
+    *dt = icar::dt_from_maxima(m, cfl, cfl_strictness, use_density);
+    if (*dt < 1e-1f)
+        return fail(h, ICAR_ADV_CFL_VIOLATION, "time step too small: dt = %g s (max |u| %g, |v| %g, |w| %g)",
+                    (double)*dt, (double)m[0], (double)m[1], (double)m[2]);
+    return ICAR_ADV_OK;
 }
 
 int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits)

@@ -44,7 +44,7 @@ typedef enum {
     ICAR_ADV_OK = 0,
     ICAR_ADV_BAD_ARG = 1,        /* invalid size, id, option combination or pointer      */
     ICAR_ADV_OOM = 2,            /* device or pinned host allocation failed              */
-    ICAR_ADV_CFL_VIOLATION = 3,  /* debug option: a Courant number >= 1 was found        */
+    ICAR_ADV_CFL_VIOLATION = 3,  /* debug: a Courant number >= 1; compute_dt: dt < 0.1 s */
     ICAR_ADV_NAN_INPUT = 4,      /* debug option: a non-finite input value was found     */
     ICAR_ADV_TIMEOUT = 5,        /* a bounded device wait gave up                        */
     ICAR_ADV_CUDA_ERROR = 6,     /* a CUDA runtime call failed                           */
@@ -173,6 +173,24 @@ int icar_adv_enforce_limits(icar_adv_t *h);
  * fields: apply_forcing(dt) -> advect(real(dt)) -> enforce_limits if
  * enforce_limits != 0.  Asynchronous on the handle's stream. */
 int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits);
+
+/* balance_uvw(domain, options), src/physics/wind.f90:88-164, called every
+ * step before advection when advect_density is set (time_step.f90:324):
+ * rebuilds the resident w from the horizontal divergence of the resident u
+ * and v (calc_divergence with horz_only, calc_w), density weighted when the
+ * handle's advect_density is set.  Columns outside its-1..ite+1 x
+ * jts-1..jte+1 get w = 0, as in the reference.  Asynchronous. */
+int icar_adv_balance_uvw(icar_adv_t *h);
+
+/* compute_dt(dx, u, v, w, rho, dz, ..., CFL, cfl_strictness, use_density),
+ * src/main/time_step.f90:51-168, on the resident winds: the largest stable
+ * step for cfl (options%time_options%cfl_reduction_factor) and
+ * cfl_strictness 1..5, with dz_levels the host array of nz level
+ * thicknesses (options%parameters%dz_levels).  Writes *dt and returns
+ * ICAR_ADV_CFL_VIOLATION when dt < 0.1 s (where the reference stops).
+ * Synchronises the handle's stream. */
+int icar_adv_compute_dt(icar_adv_t *h, const float *dz_levels, float cfl, int32_t cfl_strictness,
+                        int32_t use_density, float *dt);
 
 /* Block until the handle's stream has drained; reports device-side errors. */
 int icar_adv_sync(icar_adv_t *h);

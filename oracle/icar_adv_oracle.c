@@ -16,6 +16,8 @@
  *   src/objects/domain_obj.f90:3092-3149          enforce_limits
  *   src/objects/domain_obj.f90:3285-3400          init_relax_filters
  *   src/objects/domain_obj.f90:3457-3526          apply_forcing (advected part)
+ *   src/physics/wind.f90:88-271                   balance_uvw, calc_w, calc_divergence
+ *   src/main/time_step.f90:51-168                 compute_dt
  * The reference has no golden vectors for this path (its only MPDATA test,
  * src/tests/test_mpdata.f90, is print-only and disabled), so parity of this
  * restatement is pinned by the known-answer properties in
@@ -47,6 +49,7 @@ typedef struct {
 #define EPS15 1e-15f
 #define RK3_THIRD 0.333f
 #define RABS(a) fabsf(a)
+#define RSQRT3 sqrtf(3.0f)
 #include "oracle_body.inc"
 #undef REAL
 #undef FN
@@ -54,6 +57,7 @@ typedef struct {
 #undef EPS15
 #undef RK3_THIRD
 #undef RABS
+#undef RSQRT3
 #undef C3
 #undef UX
 
@@ -63,6 +67,7 @@ typedef struct {
 #define EPS15 1e-15
 #define RK3_THIRD 0.333
 #define RABS(a) fabs(a)
+#define RSQRT3 sqrt(3.0)
 #include "oracle_body.inc"
 #undef REAL
 #undef FN

@@ -171,3 +171,37 @@ def flux_limiter(q, q2, u2, v2, w2):
     fn = getattr(lib, "flux_limiter" + _sfx(q.dtype))
     fn.restype = None
     fn(C.c_int(nx), C.c_int(ny), C.c_int(nz), _p(q), _p(q2), _p(u2), _p(v2), _p(w2))
+
+
+def balance_uvw(case, hs: int, advect_density: int = 1, dtype=np.float32) -> np.ndarray:
+    """balance_uvw (wind.f90:88-164): w rebuilt from the horizontal
+    divergence of u, v; returns the new w (the case is not modified)."""
+    lib = load()
+    t = np.dtype(dtype)
+    ct = C.c_double if t == np.float64 else C.c_float
+    f = {k: np.ascontiguousarray(getattr(case, k), dtype=t)
+         for k in ("u", "v", "density", "jacobian_u", "jacobian_v", "jacobian_w", "advection_dz")}
+    w = np.ascontiguousarray(case.w, dtype=t).copy()
+    fn = getattr(lib, "balance_uvw" + _sfx(t))
+    fn.restype = None
+    fn(C.c_int(case.nx), C.c_int(case.ny), C.c_int(case.nz), C.c_int(hs), ct(case.dx), C.c_int(advect_density),
+       _p(f["u"]), _p(f["v"]), _p(w), _p(f["density"]), _p(f["advection_dz"]), _p(f["jacobian_u"]),
+       _p(f["jacobian_v"]), _p(f["jacobian_w"]))
+    return w
+
+
+def compute_dt(case, hs: int, dz_levels, cfl: float, strictness: int, use_density: int = 0,
+               dtype=np.float32) -> tuple[float, bool]:
+    """compute_dt (time_step.f90:51-168) on the case's winds; returns
+    (dt, too_small) where too_small is the reference's dt < 0.1 stop."""
+    lib = load()
+    t = np.dtype(dtype)
+    ct = C.c_double if t == np.float64 else C.c_float
+    u, v, w = (np.ascontiguousarray(getattr(case, k), dtype=t) for k in ("u", "v", "w"))
+    dz = np.ascontiguousarray(dz_levels, dtype=t)
+    fn = getattr(lib, "compute_dt" + _sfx(t))
+    fn.restype = ct
+    small = C.c_int(0)
+    dt = fn(C.c_int(case.nx), C.c_int(case.ny), C.c_int(case.nz), C.c_int(hs), ct(case.dx), _p(u), _p(v), _p(w),
+            _p(dz), ct(cfl), C.c_int(strictness), C.c_int(use_density), C.byref(small))
+    return float(dt), bool(small.value)

@@ -136,3 +136,80 @@ def test_golden_fixtures(oracle_lib):
         out = oracle_lib.run_steps(case, opts, case.dt, nsteps)
         for k, v in out.items():
             assert np.array_equal(v, ref[k]), (name, k)
+
+
+# ---------------------------------------------------------------- wind balance
+def _divergence3d(case, w, adv_den):
+    """calc_divergence without horz_only (wind.f90:208-271) in FP64."""
+    u, v, ju, jv, jw = (getattr(case, k).astype(np.float64) for k in ("u", "v", "jacobian_u", "jacobian_v", "jacobian_w"))
+    rho, dz, w = case.density.astype(np.float64), case.advection_dz.astype(np.float64), w.astype(np.float64)
+    if adv_den:
+        um = u.copy() * ju
+        um[:, :, 1:-1] *= (rho[:, :, :-1] + rho[:, :, 1:]) / 2
+        um[:, :, 0] *= 1.5 * rho[:, :, 0] - 0.5 * rho[:, :, 1]          # extrapolated at the edges
+        um[:, :, -1] *= 1.5 * rho[:, :, -1] - 0.5 * rho[:, :, -2]
+        vm = v.copy() * jv
+        vm[1:-1] *= (rho[:-1] + rho[1:]) / 2
+        vm[0] *= 1.5 * rho[0] - 0.5 * rho[1]
+        vm[-1] *= 1.5 * rho[-1] - 0.5 * rho[-2]
+        rho_i = (rho[:, :-1] * dz[:, :-1] + rho[:, 1:] * dz[:, 1:]) / (dz[:, :-1] + dz[:, 1:])
+        wm = w * jw
+        wm[:, :-1] *= rho_i
+        wm[:, -1] *= rho[:, -1]
+    else:
+        um, vm, wm = u * ju, v * jv, w * jw
+    div = ((um[:, :, 1:] - um[:, :, :-1]) + (vm[1:] - vm[:-1])) / case.dx
+    wb = np.concatenate([np.zeros_like(wm[:, :1]), wm[:, :-1]], axis=1)
+    return div + (wm - wb) / dz
+
+
+@pytest.mark.parametrize("adv_den", [0, 1])
+def test_balance_uvw_closes_continuity(oracle_lib, adv_den):
+    """After balance_uvw the 3-D (mass-flux) divergence vanishes in every
+    column of the region its-1..ite+1 (FP32 round-off), and w is zero in the
+    columns outside it (wind.f90:178)."""
+    O = oracle_lib
+    case = synth.config2(seed=8, nx=40, ny=33, nz=12)
+    for hs in (1, 2, 3):
+        w = O.balance_uvw(case, hs, adv_den)
+        d = _divergence3d(case, w, adv_den)
+        lo = max(hs - 1, 0)
+        ex, ey = min(case.nx - hs, case.nx - 1), min(case.ny - hs, case.ny - 1)
+        inner = d[lo:ey + 1, :-1, lo:ex + 1]          # the top level closes against the model lid flux
+        scale = np.abs(case.u).max() / case.dx
+        assert np.abs(inner).max() < 1e-5 * scale, (hs, np.abs(inner).max())
+        mask = np.ones(w.shape, bool)
+        mask[lo:ey + 1, :, lo:ex + 1] = False
+        assert not w[mask].any()
+
+
+def test_balance_uvw_reproduces_the_continuity_w(oracle_lib):
+    """Without density weighting, balancing the synthetic winds returns the
+    w they were built with (the generator integrates the same continuity)."""
+    O = oracle_lib
+    case = synth.config1(seed=4, nx=50, ny=44, nz=10)
+    w = O.balance_uvw(case, 2, 0)
+    assert np.array_equal(w[1:-1, :, 1:-1], case.w[1:-1, :, 1:-1])
+
+
+def test_compute_dt_known_answers(oracle_lib):
+    """Uniform u = 10 m/s, v = w = 0, dx = 1 km: the per-cell rate is
+    |u|/dx = 0.01 /s; the 1-D limits use |u| itself (the reference mixes the
+    two); cfl_strictness 1..5 give the documented combinations."""
+    O = oracle_lib
+    case = synth.config1(seed=0, nx=20, ny=18, nz=6)
+    case.dx = 1000.0
+    case.u[:] = 10.0
+    case.v[:] = 0.0
+    case.w[:] = 0.0
+    dz = np.full(case.nz, 500.0, np.float32)
+    f = np.float32
+    sqrt3 = f(np.sqrt(f(3.0))) * f(1.001)
+    expect = {1: f(0.9) / (f(10.0) * sqrt3), 2: f(0.9) / max(f(10.0), f(0.01) * f(0.577350269)),
+              3: f(0.9) / f(0.01), 4: f(0.9) / (f(0.01) * sqrt3), 5: f(0.9) / f(10.0)}
+    for s, dt in expect.items():
+        got, small = O.compute_dt(case, 2, dz, 0.9, s)
+        assert got == float(f(dt)), (s, got, dt)
+        assert small == (dt < f(0.1))
+    got, _ = O.compute_dt(case, 2, dz, 0.9, 3, use_density=1)
+    assert got == float("inf")
