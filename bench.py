@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="full_species",
-                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large", "wind"])
+                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large", "wind", "mp"])
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-duration", type=float, default=6.0)
     p.add_argument("--serve-steps-scale", type=float, default=0.1)
@@ -496,6 +496,72 @@ def run_wind(args):
         "clocks": clk}), flush=True)
 
 
+# ------------------------------------------------------------ microphysics
+def run_mp(args):
+    """The simple microphysics (mp_simple) on the full-species domain, timed
+    with CUDA events on the library's stream, against the HBM roofline of
+    its bytes; alone and as the advect -> mp pair with the species resident."""
+    import torch
+    from hicar_b200 import _lib as L, replicas as R, roofline, synth
+    from hicar_b200.advection import Domain, Options, PhysicsOptions, adv_init, kMP_SB04
+
+    if not R.from_env().is_root:
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    case, desc = make_case("full_species", 100)
+    synth.add_mp_fields(case)
+    opts = Options(physics=PhysicsOptions(microphysics=kMP_SB04))
+    d = Domain.from_case(case, device=local)
+    adv_init(d, opts)
+    lib = L.load()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
+    h = d.handle
+
+    def mp_call():
+        L.check(lib.icar_adv_mp_simple(h, C.c_float(case.dt)), h)
+
+    def pair():
+        L.check(lib.icar_adv_advect(h, C.c_float(case.dt)), h)
+        mp_call()
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    ms_mp = timed(mp_call, args.steps)
+    ms_pair = timed(pair, max(3, args.steps // 4))
+    clk = clocks.stop()
+    L.check(lib.icar_adv_sync(h), h)
+    d.close()
+    cells = case.cells()
+    peak, kind = roofline.hbm_peak()
+    mp_bytes = cells * 56.0     # pressure, th, exner, rho, qv, qc, qr, qs, dz read; th, qv, qc, qr, qs written
+    print(json.dumps({
+        "metric": "simple microphysics cells/s", "value": cells / (ms_mp / 1e3), "unit": "cells/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mp, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "mp_simple (SB04) on the " + desc + " (qv x1.5, hydrostatic pressure)"},
+        "roofline": {"kernel": "k_mp_simple", "bound": "hbm", "achieved": mp_bytes / (ms_mp / 1e3) / 1e9,
+                     "peak": peak, "unit": "GB/s", "frac": mp_bytes / (ms_mp / 1e3) / 1e9 / peak, "traffic": None,
+                     "peak_kind": kind, "algorithmic_bytes_per_launch": mp_bytes,
+                     "bytes_model": "56 B per cell: nine fields read and five written once"},
+        "advect_then_mp_ms": ms_pair, "clocks": clk}), flush=True)
+
+
 # ------------------------------------------------------------ ensemble
 ENSEMBLE_DESC = ("batched uneven ensemble: 64 independent domains, nx,ny ~ U[64,384], nz ~ U[20,50], "
                  "12 fields each, dt 20 s, one graph launch per step vs 64 plain launches")
@@ -719,6 +785,8 @@ def main():
         run_large(args)
     elif args.workload == "wind":
         run_wind(args)
+    elif args.workload == "mp":
+        run_mp(args)
     else:
         run_b200(args)
 

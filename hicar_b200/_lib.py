@@ -16,16 +16,17 @@ LIB_PATH = Path(__file__).resolve().parent / "libicar_adv.so"
 MAX_SPECIES = 32
 
 # status codes (icar_adv_status)
-OK, BAD_ARG, OOM, CFL_VIOLATION, NAN_INPUT, TIMEOUT, CUDA_ERROR, NOT_READY, OVER_BUDGET = range(9)
+OK, BAD_ARG, OOM, CFL_VIOLATION, NAN_INPUT, TIMEOUT, CUDA_ERROR, NOT_READY, OVER_BUDGET, PHYSICS_STOP = range(10)
 STATUS_NAMES = {
     0: "OK", 1: "BAD_ARG", 2: "OOM", 3: "CFL_VIOLATION", 4: "NAN_INPUT", 5: "TIMEOUT",
-    6: "CUDA_ERROR", 7: "NOT_READY", 8: "OVER_BUDGET",
+    6: "CUDA_ERROR", 7: "NOT_READY", 8: "OVER_BUDGET", 9: "PHYSICS_STOP",
 }
 
 # field ids (kVARS numbering, src/constants/icar_constants.f90)
 F_U, F_V, F_W = 1, 2, 3
 F_THETA, F_QV, F_QC, F_NC, F_QI, F_NI, F_QR, F_NR, F_QS, F_NS, F_QG, F_NG = 7, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19
 F_DENSITY, F_DZ_INTERFACE = 39, 43
+F_PRESSURE, F_EXNER, F_DZ_MASS = 5, 37, 42
 F_JACOBIAN, F_JACOBIAN_U, F_JACOBIAN_V, F_JACOBIAN_W, F_ADVECTION_DZ, F_RELAX_FILTER = 1001, 1002, 1003, 1004, 1005, 1006
 F_FORCING_BASE, F_DQDT_BASE = 2000, 3000
 
@@ -99,6 +100,9 @@ _PROTOS = {
     "icar_adv_balance_uvw": (C.c_int, [C.c_void_p]),
     "icar_adv_compute_dt": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_float, C.c_int32, C.c_int32,
                                       C.POINTER(C.c_float)]),
+    "icar_adv_mp_simple": (C.c_int, [C.c_void_p, C.c_float]),
+    "icar_adv_get_precipitation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "icar_adv_set_precipitation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "icar_adv_set_tile_shape": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_set_species_group": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),

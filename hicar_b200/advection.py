@@ -29,6 +29,7 @@ from . import _lib as L
 kADV_STD = 1
 kADV_MPDATA = 2
 kFLUXCOR_MONO = 1
+kMP_SB04 = 2          # physics%microphysics, icar_constants.f90:393
 
 
 @dataclass
@@ -44,6 +45,7 @@ class AdvOptions:                      # adv_options_type, opt_types.f90:119-127
 @dataclass
 class PhysicsOptions:
     advection: int = kADV_MPDATA
+    microphysics: int = 0
 
 
 @dataclass
@@ -80,6 +82,8 @@ _METRIC_FIELDS = {
     "u": L.F_U, "v": L.F_V, "w": L.F_W, "density": L.F_DENSITY, "jacobian": L.F_JACOBIAN,
     "jacobian_u": L.F_JACOBIAN_U, "jacobian_v": L.F_JACOBIAN_V, "jacobian_w": L.F_JACOBIAN_W,
     "advection_dz": L.F_ADVECTION_DZ,
+    # read only by the simple microphysics (mp)
+    "pressure": L.F_PRESSURE, "exner": L.F_EXNER, "dz_mass": L.F_DZ_MASS,
 }
 
 
@@ -98,6 +102,7 @@ class Domain:
         self.north_boundary, self.south_boundary, self.east_boundary, self.west_boundary = boundaries
         self.u = self.v = self.w = self.density = None
         self.jacobian = self.jacobian_u = self.jacobian_v = self.jacobian_w = self.advection_dz = None
+        self.pressure = self.exner = self.dz_mass = None
         self.adv_vars: dict[str, np.ndarray] = {}
         self.forcing: dict[str, tuple[np.ndarray, np.ndarray | None]] = {}
         self._h = None
@@ -107,7 +112,8 @@ class Domain:
     def from_case(cls, case, device: int = 0) -> "Domain":
         d = cls(case.nx, case.ny, case.nz, case.dx, device=device)
         for k in _METRIC_FIELDS:
-            setattr(d, k, np.ascontiguousarray(getattr(case, k), np.float32))
+            a = getattr(case, k, None)
+            setattr(d, k, None if a is None else np.ascontiguousarray(a, np.float32))
         d.adv_vars = {k: np.ascontiguousarray(v, np.float32).copy() for k, v in case.species.items()}
         return d
 
@@ -132,6 +138,8 @@ class Domain:
         d._h = h
         d._options = options
         for k, fid in _METRIC_FIELDS.items():
+            if fields.get(k) is None:
+                continue                     # the microphysics inputs are optional
             L.check(lib.icar_adv_set_field_device(h, fid, C.c_void_p(fields[k].data_ptr())), h)
         for k in names:
             t = fields["species"][k]
@@ -339,6 +347,27 @@ def compute_dt(domain: Domain, options: Options, dz_levels, use_density: bool = 
                                          C.c_float(t.cfl_reduction_factor), int(t.cfl_strictness),
                                          int(bool(use_density)), C.byref(out)), domain.handle)
     return float(out.value)
+
+
+def mp(domain: Domain, options: Options, dt: float) -> None:
+    """mp_driver.f90:813 mp(domain, options, dt) for physics%microphysics =
+    kMP_SB04 (mp_simple): theta, qv, qc, qr, qs must be advected species of
+    the domain and pressure, exner, density and dz_mass set.  Asynchronous;
+    the accumulated rain and snow are read with precipitation()."""
+    if options.physics.microphysics != kMP_SB04:
+        raise NotImplementedError("only the simple microphysics (kMP_SB04) runs on the device")
+    domain._flush()
+    L.check(L.load().icar_adv_mp_simple(domain.handle, C.c_float(dt)), domain.handle)
+
+
+def precipitation(domain: Domain) -> tuple[np.ndarray, np.ndarray]:
+    """The real64 accumulated_precipitation and accumulated_snowfall (ny, nx)
+    the microphysics has added up on the device."""
+    rain = np.zeros((domain.ny, domain.nx), np.float64)
+    snow = np.zeros((domain.ny, domain.nx), np.float64)
+    L.check(L.load().icar_adv_get_precipitation(domain.handle, rain.ctypes.data_as(C.c_void_p),
+                                                snow.ctypes.data_as(C.c_void_p)), domain.handle)
+    return rain, snow
 
 
 def step(domain: Domain, options: Options, dt_seconds: float, enforce_limits: bool = False) -> None:

@@ -24,6 +24,7 @@
 #include "std_kernels.cuh"
 #include "batch_kernels.cuh"
 #include "wind_kernels.cuh"
+#include "mp_kernels.cuh"
 
 using icar::Geo;
 
@@ -65,6 +66,13 @@ struct icar_adv_domain {
     DevBuf q1, u2, v2, w2, u2l, v2l, w2l;      // MPDATA staged scratch
     DevBuf Gc, DJR, Wp;                        // fused path: J*rho, dz*J*rho, W_m/dz
     DevBuf dtbuf;                              // compute_dt: 4 maxima then dz_levels (nz)
+    // simple microphysics: its extra resident fields, the real64 rain and
+    // snow accumulations (nx*ny each) and the device stop flag
+    DevBuf pressure, exner, dz_mass;
+    bool have_pressure = false, have_exner = false, have_dz_mass = false;
+    double *acc_precip = nullptr;             // rain [0, nx*ny), snow [nx*ny, 2*nx*ny)
+    int *mp_stop = nullptr;
+    bool mp_ran = false;
     std::vector<DevBuf> qn, q1s;               // fused path: next state and pass-1 result per species
     bool fused_ready = false;
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
@@ -316,6 +324,14 @@ int resolve(icar_adv_t *h, int field, FieldRef &r)
     case ICAR_F_JACOBIAN_W: r = {&h->jac_w, nx, ny, nz, &h->have_jac_w}; return ICAR_ADV_OK;
     case ICAR_F_ADVECTION_DZ: r = {&h->dz, nx, ny, nz, &h->have_dz}; return ICAR_ADV_OK;
     case ICAR_F_RELAX_FILTER: r = FieldRef{}; r.ex = nx; r.ey = ny; r.ez = 1; r.is_filter = true; return ICAR_ADV_OK;
+    case ICAR_F_PRESSURE: case ICAR_F_EXNER: case ICAR_F_DZ_MASS: {
+        DevBuf *b = field == ICAR_F_PRESSURE ? &h->pressure : field == ICAR_F_EXNER ? &h->exner : &h->dz_mass;
+        bool *f = field == ICAR_F_PRESSURE ? &h->have_pressure : field == ICAR_F_EXNER ? &h->have_exner : &h->have_dz_mass;
+        int e = alloc(h, *b, h->n_cell);
+        if (e) return e;
+        r = {b, nx, ny, nz, f};
+        return ICAR_ADV_OK;
+    }
     default: break;
     }
     int base = field;
@@ -415,6 +431,21 @@ int copy_field(icar_adv_t *h, int field, float *host, const int64_t *strides, bo
 }
 
 inline unsigned blocks_for(size_t n, unsigned bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// After a sync: report (once) a column where mp_simple reached the
+// reference's stop condition.
+int check_mp_stop(icar_adv_t *h)
+{
+    if (!h->mp_ran || !h->mp_stop) return ICAR_ADV_OK;
+    int flag = 0;
+    cudaError_t e = cudaMemcpy(&flag, h->mp_stop, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "reading the mp stop flag: %s", cudaGetErrorString(e));
+    h->mp_ran = false;
+    if (!flag) return ICAR_ADV_OK;
+    cudaMemset(h->mp_stop, 0, sizeof(int));
+    return fail(h, ICAR_ADV_PHYSICS_STOP,
+                "mp_simple: phase_change left a hydrometeor in [-1e-30, 0), where the reference stops");
+}
 
 int check_launch(icar_adv_t *h, const char *what, int n = 1)
 {
@@ -799,8 +830,10 @@ int icar_adv_destroy(icar_adv_t *h)
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
                       &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
                       &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp, &h->Gc,
-                      &h->DJR, &h->Wp, &h->dtbuf})
+                      &h->DJR, &h->Wp, &h->dtbuf, &h->pressure, &h->exner, &h->dz_mass})
         release(*b);
+    if (h->acc_precip) cudaFree(h->acc_precip);
+    if (h->mp_stop) cudaFree(h->mp_stop);
     for (auto &b : h->q) release(b);
     for (auto &b : h->qn) release(b);
     for (auto &b : h->q1s) release(b);
@@ -958,6 +991,82 @@ int icar_adv_compute_dt(icar_adv_t *h, const float *dz_levels, float cfl, int32_
     return ICAR_ADV_OK;
 }
 
+int icar_adv_mp_simple(icar_adv_t *h, float dt)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (h->batch) return fail(h, ICAR_ADV_BAD_ARG, "domain is a batch member");
+    if (!(dt >= 0.0f) || !std::isfinite(dt)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite and >= 0");
+    cudaSetDevice(h->desc.device);
+    const int s_th = species_slot(h, ICAR_F_THETA), s_qv = species_slot(h, ICAR_F_QV),
+              s_qc = species_slot(h, ICAR_F_QC), s_qr = species_slot(h, ICAR_F_QR), s_qs = species_slot(h, ICAR_F_QS);
+    if (s_th < 0 || s_qv < 0 || s_qc < 0 || s_qr < 0 || s_qs < 0)
+        return fail(h, ICAR_ADV_BAD_ARG, "mp_simple needs theta, qv, qc, qr and qs among the domain's fields");
+    const char *missing = nullptr;
+    if (!h->have_pressure) missing = "pressure";
+    else if (!h->have_exner) missing = "exner";
+    else if (!h->have_dz_mass) missing = "dz (dz_mass)";
+    else if (!h->have_rho) missing = "density";
+    else
+        for (int s : {s_th, s_qv, s_qc, s_qr, s_qs})
+            if (!h->have_q[s]) missing = "a microphysics species";
+    if (missing) return fail(h, ICAR_ADV_NOT_READY, "field %s was never set", missing);
+    const Geo &g = h->g;
+    if (g.nz > 512) return fail(h, ICAR_ADV_BAD_ARG, "mp_simple supports at most 512 levels");
+    const size_t n2 = (size_t)g.nx * g.ny;
+    if (!h->acc_precip) {
+        CUDA_TRY(h, cudaMalloc(&h->acc_precip, 2 * n2 * sizeof(double)));
+        CUDA_TRY(h, cudaMemsetAsync(h->acc_precip, 0, 2 * n2 * sizeof(double), h->stream));
+    }
+    if (!h->mp_stop) {
+        CUDA_TRY(h, cudaMalloc(&h->mp_stop, sizeof(int)));
+        CUDA_TRY(h, cudaMemsetAsync(h->mp_stop, 0, sizeof(int), h->stream));
+    }
+    // the time constants of this dt, in the reference's FP32 (mp_simple.f90:618-622)
+    const float cloud2snow = std::exp(-1.0f * (1.0f / 2000.0f) * dt);
+    const float cloud2rain = std::exp(-1.0f * (1.0f / 500.0f) * dt);
+    const int hs = h->hs;
+    const size_t ncol = (size_t)std::max(g.nx - 2 * hs, 0) * (size_t)std::max(g.ny - 2 * hs, 0);
+    if (ncol > 0)
+        icar::k_mp_simple<<<blocks_for(ncol, 128), 128, 0, h->stream>>>(
+            g, hs, dt, cloud2rain, cloud2snow, h->pressure.p, h->q[s_th].p, h->exner.p, h->rho.p, h->q[s_qv].p,
+            h->q[s_qc].p, h->q[s_qr].p, h->q[s_qs].p, h->dz_mass.p, h->acc_precip, h->acc_precip + n2, h->mp_stop);
+    h->mp_ran = true;
+    return check_launch(h, "mp_simple");
+}
+
+int icar_adv_get_precipitation(icar_adv_t *h, double *rain, double *snow)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    const size_t n2 = (size_t)h->g.nx * h->g.ny;
+    if (!h->acc_precip) {
+        if (rain) std::fill(rain, rain + n2, 0.0);
+        if (snow) std::fill(snow, snow + n2, 0.0);
+        return ICAR_ADV_OK;
+    }
+    if (rain) CUDA_TRY(h, cudaMemcpyAsync(rain, h->acc_precip, n2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (snow)
+        CUDA_TRY(h, cudaMemcpyAsync(snow, h->acc_precip + n2, n2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return icar_adv_sync(h);
+}
+
+int icar_adv_set_precipitation(icar_adv_t *h, const double *rain, const double *snow)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    cudaSetDevice(h->desc.device);
+    const size_t n2 = (size_t)h->g.nx * h->g.ny;
+    if (!h->acc_precip) CUDA_TRY(h, cudaMalloc(&h->acc_precip, 2 * n2 * sizeof(double)));
+    for (int part = 0; part < 2; part++) {
+        const double *src = part == 0 ? rain : snow;
+        double *dst = h->acc_precip + part * n2;
+        if (src)
+            CUDA_TRY(h, cudaMemcpyAsync(dst, src, n2 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        else
+            CUDA_TRY(h, cudaMemsetAsync(dst, 0, n2 * sizeof(double), h->stream));
+    }
+    return icar_adv_sync(h);
+}
+
 int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits)
 {
     int e = icar_adv_apply_forcing(h, dt_seconds);
@@ -974,7 +1083,7 @@ int icar_adv_sync(icar_adv_t *h)
     cudaSetDevice(h->desc.device);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "stream sync: %s", cudaGetErrorString(e));
-    return ICAR_ADV_OK;
+    return check_mp_stop(h);
 }
 
 int icar_adv_set_stream(icar_adv_t *h, void *cuda_stream)

@@ -1,0 +1,238 @@
+// Simple microphysics (SB04) on the device: mp_simple_driver,
+// src/physics/mp_simple.f90:595-646, the scheme mp_driver.f90:548-568 runs
+// after advection when physics%microphysics = kMP_SB04.
+//
+// k_mp_simple: one thread per column of the tile (its..ite x jts..jte).
+// Phase 1 walks up the column doing the per-level conversions
+// (mp_conversions: saturation adjustment by the reference's iteration,
+// autoconversion, melting, evaporation and sublimation with latent-heat
+// feedback) and leaves the air temperature T = th*pii in the th array.
+// Phases 2 and 3 sediment rain and then snow in CFL substeps (sediment, as a
+// single upward sweep: each level's downward flux is formed from the level
+// above before that level is touched, exactly the reference's values and
+// order) with the evaporation/sublimation of what fell into unsaturated
+// levels.  Phase 4 turns T back into th.  The column's rain and snow are
+// added to the real64 accumulations (one writer per column).
+//
+// Arithmetic follows the reference expression by expression (no FMA
+// contraction).  The one transcendental, exp in sat_mr, is evaluated as the
+// float rounding of a double-precision exp: the correctly rounded
+// single-precision exp except within about 2^-29 ulp of a halfway point.
+// The CPU restatement evaluates it the same way; the reference's libm expf
+// may differ from it in the last bit in near-halfway cases.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace icar {
+namespace mps {
+constexpr float LH_VAPOR = 2.26E6f, DLHVDT = 2400.0f, LH_LIQUID = 3.34E5f, HEAT_CAPACITY = 1006.0f;
+constexpr float SMALL = 1E-30f, FREEZING = 273.15f;
+constexpr float SNOW_FALL = 1.5f, RAIN_FALL = 10.0f, SNOW_INIT = 0.0001f, RAIN_INIT = 0.0001f;
+}  // namespace mps
+
+// sat_mr, mp_simple.f90:146-182
+__device__ __forceinline__ float mp_sat_mr(float temperature, float pressure)
+{
+    float a, b;
+    if (temperature < mps::FREEZING) {
+        a = 21.8745584f;
+        b = 7.66f;
+    } else {
+        a = 17.2693882f;
+        b = 35.86f;
+    }
+    float e_s = 610.78f * __double2float_rn(exp((double)(a * (temperature - 273.16f) / (temperature - b))));
+    if ((pressure - e_s) <= 0.0f) e_s = pressure * 0.99999f;
+    return 0.6219907f * e_s / (pressure - e_s);
+}
+
+// cloud_conversion, mp_simple.f90:198-280 (its diagnostic prints omitted)
+__device__ __forceinline__ void mp_cloud_conversion(float pressure, float &temperature, float &qv, float &qc,
+                                                    float &qvsat)
+{
+    const float maxerr = 1e-4f;
+    int iteration = 0;
+    float lastqv = qv + maxerr * 2.0f;
+    const float vapor2temp = (mps::LH_VAPOR + (373.15f - temperature) * mps::DLHVDT) / mps::HEAT_CAPACITY;
+    const float pre_qc = qc, pre_t = temperature;
+    while ((fabsf(lastqv - qv) > maxerr) && (iteration < 15)) {
+        iteration = iteration + 1;
+        lastqv = qv;
+        qvsat = mp_sat_mr(temperature, pressure);
+        if (qv > qvsat) {
+            const float excess = (qv - qvsat) * 0.5f;
+            temperature = temperature + (excess * vapor2temp);
+            qv = qv - excess;
+            qc = qc + excess;
+        } else if (qc > 0.0f) {
+            const float excess = (qvsat - qv) * 0.5f;
+            if (excess < qc) {
+                temperature = temperature - (excess * vapor2temp);
+                qv = qv + excess;
+                qc = qc - excess;
+            } else {
+                qv = qv + qc;
+                temperature = temperature - (qc * vapor2temp);
+                qc = 0.0f;
+            }
+        }
+    }
+    if (iteration == 15) {
+        qv = mp_sat_mr(pre_t, pressure);
+        temperature = pre_t;
+        qc = pre_qc;
+    }
+    qc = fmax_(qc, 0.0f);
+}
+
+// cloud2hydrometeor, mp_simple.f90:295-315
+__device__ __forceinline__ void mp_cloud2hydrometeor(float &qc, float &q, float conversion, float qcmin)
+{
+    const float delta = qc > qcmin ? qc - (qc * conversion) : 0.0f;
+    if (delta < qc) {
+        qc = qc - delta;
+        q = q + delta;
+    } else {
+        q = q + qc;
+        qc = 0.0f;
+    }
+    qc = fmax_(qc, 0.0f);
+}
+
+// phase_change, mp_simple.f90:333-362; stop is set where the reference
+// stops the program (q1 left in [-1e-30, 0))
+__device__ __forceinline__ void mp_phase_change(float &temperature, float &q1, float qmax, float &q2, float Lheat,
+                                                float change_rate, int &stop)
+{
+    const float mass2temp = Lheat / mps::HEAT_CAPACITY;
+    float delta = (qmax - q2) * change_rate;
+    if (delta > q1) delta = q1;
+    if (delta > ((qmax - q2) * 0.99f)) delta = (qmax - q2) * 0.99f;
+    q1 = q1 - delta;
+    if (q1 < 0.0f) {
+        if ((q1 + mps::SMALL) < 0.0f)
+            q1 = 0.0f;
+        else
+            stop = 1;
+    }
+    q2 = q2 + delta;
+    temperature = temperature + delta * mass2temp;
+}
+
+// mp_conversions, mp_simple.f90:381-420
+__device__ __forceinline__ void mp_conversions(float pressure, float &temperature, float &qv, float &qc, float &qr,
+                                               float &qs, float cloud2rain, float cloud2snow, int &stop)
+{
+    const float L_melt = -1.0f * mps::LH_LIQUID;
+    const float L_evap = -1.0f * (mps::LH_VAPOR + (373.15f - temperature) * mps::DLHVDT);
+    const float L_subl = L_melt + L_evap;
+    float qvsat = 0.0f;
+    mp_cloud_conversion(pressure, temperature, qv, qc, qvsat);
+    if ((qc + qr + qs) > mps::SMALL) {
+        if (qc > mps::SMALL) {
+            if (temperature > mps::FREEZING) {
+                mp_cloud2hydrometeor(qc, qr, cloud2rain, mps::RAIN_INIT);
+                if (qs > mps::SMALL) mp_phase_change(temperature, qs, 100.0f, qr, L_melt, cloud2rain, stop);
+            } else {
+                mp_cloud2hydrometeor(qc, qs, cloud2snow, mps::SNOW_INIT);
+            }
+        }
+        if (qv < qvsat) {
+            if (qr > mps::SMALL) mp_phase_change(temperature, qr, qvsat, qv, L_evap, cloud2rain / 2.0f, stop);
+            if (qs > mps::SMALL) mp_phase_change(temperature, qs, qvsat, qv, L_subl, cloud2snow / 2.0f, stop);
+        }
+    }
+}
+
+// One column.  T lives in th between the phases.
+__global__ void k_mp_simple(Geo g, int hs, float dt, float cloud2rain, float cloud2snow,
+                            const float *__restrict__ pressure, float *__restrict__ th,
+                            const float *__restrict__ pii, const float *__restrict__ rho, float *__restrict__ qv,
+                            float *__restrict__ qc, float *__restrict__ qr, float *__restrict__ qs,
+                            const float *__restrict__ dz, double *__restrict__ acc_rain,
+                            double *__restrict__ acc_snow, int *__restrict__ stop_flag)
+{
+    const int ti = g.nx - 2 * hs;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti <= 0 || t >= (size_t)ti * (size_t)(g.ny - 2 * hs)) return;
+    const int i = hs + (int)(t % (size_t)ti), j = hs + (int)(t / (size_t)ti);
+    const int nz = g.nz;
+    const size_t st = (size_t)g.P, c0 = ix(g, i, 0, j);
+    int stop = 0;
+    // phase 1: conversions level by level
+    for (int k = 0; k < nz; k++) {
+        const size_t c = c0 + k * st;
+        float T = th[c] * pii[c];
+        float v = qv[c], cw = qc[c], r = qr[c], s = qs[c];
+        mp_conversions(pressure[c], T, v, cw, r, s, cloud2rain, cloud2snow, stop);
+        th[c] = T;
+        qv[c] = v;
+        qc[c] = cw;
+        qr[c] = r;
+        qs[c] = s;
+    }
+    float rain = 0.0f, snow = 0.0f;
+    // phases 2 and 3: sedimentation of rain, then of snow
+    for (int pass = 0; pass < 2; pass++) {
+        float *__restrict__ q = pass == 0 ? qr : qs;
+        const float fall = pass == 0 ? mps::RAIN_FALL : mps::SNOW_FALL;
+        float mx = q[c0];
+        for (int k = 1; k < nz; k++) mx = fmax_(mx, q[c0 + k * st]);
+        if (!(mx > mps::SMALL)) continue;
+        float m = dt / dz[c0] * fall;
+        for (int k = 1; k < nz; k++) m = fmax_(m, dt / dz[c0 + k * st] * fall);
+        const float cfl = ceilf(m);
+        const float fall_rate = dt * fall / cfl;
+        const int nsub = (int)lrintf(cfl);
+        const float rate = (pass == 0 ? cloud2rain : cloud2snow) / (float)(2 * nsub);
+        for (int sub = 0; sub < nsub; sub++) {
+            // sediment: out of the bottom level, then one sweep of the
+            // downward fluxes between levels i+1 -> i
+            float qi = q[c0];
+            const float sed = fall_rate * qi * rho[c0];
+            qi = qi - (sed / dz[c0] / rho[c0]);
+            for (int k = 0; k < nz - 1; k++) {
+                const size_t c = c0 + k * st, cu = c + st;
+                float qu = q[cu];
+                const float ru = rho[cu];
+                const float flux = fall_rate * qu * ru;
+                qi = qi + flux / (rho[c] * dz[c]);
+                qu = qu - flux / (ru * dz[cu]);
+                q[c] = qi;
+                qi = qu;
+            }
+            q[c0 + (size_t)(nz - 1) * st] = qi;
+            if (pass == 0) {
+                rain = rain + sed;
+            } else {
+                snow = snow + sed;
+                rain = rain + sed;
+            }
+            // evaporate / sublimate what reached unsaturated levels
+            for (int k = 0; k < nz; k++) {
+                const size_t c = c0 + k * st;
+                float T = th[c];
+                const float L_evap = -1.0f * (mps::LH_VAPOR + (373.15f - T) * mps::DLHVDT);
+                const float qvsat = mp_sat_mr(T, pressure[c]);
+                float v = qv[c], h = q[c];
+                if (v < qvsat && h > mps::SMALL) {
+                    mp_phase_change(T, h, qvsat, v, pass == 0 ? L_evap : -1.0f * mps::LH_LIQUID + L_evap, rate,
+                                    stop);
+                    th[c] = T;
+                    qv[c] = v;
+                    q[c] = h;
+                }
+            }
+        }
+    }
+    // phase 4: back to potential temperature
+    for (int k = 0; k < nz; k++) th[c0 + k * st] = th[c0 + k * st] / pii[c0 + k * st];
+    const size_t c2 = (size_t)i + (size_t)g.nx * j;
+    acc_rain[c2] = acc_rain[c2] + (double)rain;
+    acc_snow[c2] = acc_snow[c2] + (double)snow;
+    if (stop) atomicOr(stop_flag, 1);
+}
+
+}  // namespace icar

@@ -49,6 +49,10 @@ class Case:
     z: np.ndarray                  # cell-centre height (m)
     species: dict = field(default_factory=dict)   # name -> (ny, nz, nx)
     dt: float = 20.0
+    # simple-microphysics inputs (add_mp_fields), (ny, nz, nx)
+    pressure: np.ndarray | None = None
+    exner: np.ndarray | None = None
+    dz_mass: np.ndarray | None = None
 
     def cells(self) -> int:
         return self.nx * self.ny * self.nz
@@ -407,3 +411,20 @@ def device_config5(seed: int = 0, nx: int = 2048, ny: int = 2048, nz: int = 60, 
     host would take minutes and tens of GB of host memory."""
     return device_member(nx, ny, nz, seed, device=device, dx=250.0, dz=350.0, terrain_kind="fractal", U=15.0,
                          noise=0.05, dt=1.0, rms=800.0, hmax=4000.0)
+
+
+def add_mp_fields(case: Case, moist: float = 1.5, seed: int = 0) -> Case:
+    """Give a case the fields the simple microphysics reads: hydrostatic
+    pressure from the cell heights (scale height 8 km, 1013.25 hPa at sea
+    level), the exner function (p/1000 hPa)^(R/cp), dz_mass = the physical
+    layer thickness (advection_dz * jacobian), and qv scaled by `moist` so
+    some layers are supersaturated.  Rain and snow need qr/qs among the
+    species (config 2 and the ensemble members carry all 12)."""
+    z = case.z.astype(np.float64)
+    p = 101325.0 * np.exp(-z / 8000.0)
+    case.pressure = p.astype(F32)
+    case.exner = ((p / 100000.0) ** (287.058 / 1004.5)).astype(F32)
+    case.dz_mass = (case.advection_dz * case.jacobian).astype(F32)
+    if "qv" in case.species:
+        case.species["qv"] = (case.species["qv"] * F32(moist)).astype(F32)
+    return case

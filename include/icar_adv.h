@@ -49,7 +49,8 @@ typedef enum {
     ICAR_ADV_TIMEOUT = 5,        /* a bounded device wait gave up                        */
     ICAR_ADV_CUDA_ERROR = 6,     /* a CUDA runtime call failed                           */
     ICAR_ADV_NOT_READY = 7,      /* a field the step needs was never set                 */
-    ICAR_ADV_OVER_BUDGET = 8     /* admission refused: the memory budget would be exceeded */
+    ICAR_ADV_OVER_BUDGET = 8,    /* admission refused: the memory budget would be exceeded */
+    ICAR_ADV_PHYSICS_STOP = 9    /* a physics routine met a condition where the reference stops */
 } icar_adv_status;
 
 /* Field ids.  Model variables use the reference's kVARS numbering
@@ -74,7 +75,10 @@ enum {
     ICAR_F_ICE1_A = 20, ICAR_F_ICE1_C = 21, ICAR_F_ICE2_MASS = 22, ICAR_F_ICE2_NUMBER = 23,
     ICAR_F_ICE2_A = 24, ICAR_F_ICE2_C = 25, ICAR_F_ICE3_MASS = 26, ICAR_F_ICE3_NUMBER = 27,
     ICAR_F_ICE3_A = 28, ICAR_F_ICE3_C = 29,
+    ICAR_F_PRESSURE = 5,         /* kVARS%pressure (nx, nz, ny), simple microphysics */
+    ICAR_F_EXNER = 37,           /* kVARS%exner (nx, nz, ny), simple microphysics */
     ICAR_F_DENSITY = 39,
+    ICAR_F_DZ_MASS = 42,         /* kVARS%dz = domain%dz_mass (nx, nz, ny), simple microphysics */
     ICAR_F_DZ_INTERFACE = 43,
     ICAR_F_JACOBIAN = 1001,      /* domain%jacobian   (nx, nz, ny)   */
     ICAR_F_JACOBIAN_U = 1002,    /* domain%jacobian_u (nx+1, nz, ny) */
@@ -191,6 +195,22 @@ int icar_adv_balance_uvw(icar_adv_t *h);
  * Synchronises the handle's stream. */
 int icar_adv_compute_dt(icar_adv_t *h, const float *dz_levels, float cfl, int32_t cfl_strictness,
                         int32_t use_density, float *dt);
+
+/* mp(domain, options, dt) with physics%microphysics = kMP_SB04:
+ * mp_simple_driver, src/physics/mp_simple.f90:595-646, as
+ * src/physics/mp_driver.f90:548-568 calls it, on the resident fields:
+ * potential temperature, qv, qc, qr and qs must be among the domain's
+ * species, and pressure, exner, density and dz (dz_mass) set.  Works on
+ * the tile its..ite x jts..jte, every level; the column rain and snow of the
+ * call are added to the handle's real64 accumulations (accumulated_
+ * precipitation, accumulated_snowfall), which start at zero.  Asynchronous;
+ * the next sync reports ICAR_ADV_PHYSICS_STOP if a column met the
+ * reference's stop in phase_change. */
+int icar_adv_mp_simple(icar_adv_t *h, float dt);
+/* Copy the real64 accumulations (nx*ny each, x fastest; either may be
+ * NULL) to the host, or set them (NULL = zero).  Synchronous. */
+int icar_adv_get_precipitation(icar_adv_t *h, double *rain, double *snow);
+int icar_adv_set_precipitation(icar_adv_t *h, const double *rain, const double *snow);
 
 /* Block until the handle's stream has drained; reports device-side errors. */
 int icar_adv_sync(icar_adv_t *h);

@@ -18,6 +18,8 @@
  *   src/objects/domain_obj.f90:3457-3526          apply_forcing (advected part)
  *   src/physics/wind.f90:88-271                   balance_uvw, calc_w, calc_divergence
  *   src/main/time_step.f90:51-168                 compute_dt
+ *   src/physics/mp_simple.f90:146-646             simple microphysics (SB04)
+ *   src/physics/mp_driver.f90:477-481,548-568,741-749  its driver call and accumulation
  * The reference has no golden vectors for this path (its only MPDATA test,
  * src/tests/test_mpdata.f90, is print-only and disabled), so parity of this
  * restatement is pinned by the known-answer properties in
@@ -50,6 +52,7 @@ typedef struct {
 #define RK3_THIRD 0.333f
 #define RABS(a) fabsf(a)
 #define RSQRT3 sqrtf(3.0f)
+#define REXP(x) ((float)exp((double)(x)))  /* correctly rounded expf, see mp_simple below */
 #include "oracle_body.inc"
 #undef REAL
 #undef FN
@@ -58,6 +61,7 @@ typedef struct {
 #undef RK3_THIRD
 #undef RABS
 #undef RSQRT3
+#undef REXP
 #undef C3
 #undef UX
 
@@ -68,6 +72,7 @@ typedef struct {
 #define RK3_THIRD 0.333
 #define RABS(a) fabs(a)
 #define RSQRT3 sqrt(3.0)
+#define REXP(x) exp(x)
 #include "oracle_body.inc"
 #undef REAL
 #undef FN

@@ -205,3 +205,25 @@ def compute_dt(case, hs: int, dz_levels, cfl: float, strictness: int, use_densit
     dt = fn(C.c_int(case.nx), C.c_int(case.ny), C.c_int(case.nz), C.c_int(hs), ct(case.dx), _p(u), _p(v), _p(w),
             _p(dz), ct(cfl), C.c_int(strictness), C.c_int(use_density), C.byref(small))
     return float(dt), bool(small.value)
+
+
+def mp_simple(fields: dict, dt: float, hs: int, acc_rain=None, acc_snow=None, dtype=np.float32):
+    """mp_simple_driver (mp_simple.f90:595-646) on copies of the fields
+    (Fortran layout (ny, nz, nx)): pressure, th, pii, rho, qv, qc, qr, qs, dz.
+    Returns (updated dict of th, qv, qc, qr, qs, acc_rain, acc_snow, stop)."""
+    lib = load()
+    t = np.dtype(dtype)
+    ct = C.c_double if t == np.float64 else C.c_float
+    ny, nz, nx = fields["th"].shape
+    f = {k: np.ascontiguousarray(fields[k], dtype=t).copy() for k in ("pressure", "th", "pii", "rho", "qv", "qc",
+                                                                     "qr", "qs", "dz")}
+    ar = np.zeros((ny, nx)) if acc_rain is None else np.ascontiguousarray(acc_rain, np.float64).copy()
+    asn = np.zeros((ny, nx)) if acc_snow is None else np.ascontiguousarray(acc_snow, np.float64).copy()
+    fn = getattr(lib, "mp_simple_driver" + _sfx(t))
+    fn.restype = C.c_int
+    stop = fn(C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_int(hs), ct(dt), _p(f["pressure"]), _p(f["th"]),
+              _p(f["pii"]), _p(f["rho"]), _p(f["qv"]), _p(f["qc"]), _p(f["qr"]), _p(f["qs"]), _p(ar), _p(asn),
+              _p(f["dz"]))
+    out = {k: f[k] for k in ("th", "qv", "qc", "qr", "qs")}
+    out.update(acc_rain=ar, acc_snow=asn, stop=bool(stop))
+    return out

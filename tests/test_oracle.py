@@ -213,3 +213,59 @@ def test_compute_dt_known_answers(oracle_lib):
         assert small == (dt < f(0.1))
     got, _ = O.compute_dt(case, 2, dz, 0.9, 3, use_density=1)
     assert got == float("inf")
+
+
+# ---------------------------------------------------------------- simple microphysics
+def _mp_inputs(seed=3, nx=40, ny=36, nz=20, moist=1.5):
+    c = synth.add_mp_fields(synth.config2(seed=seed, nx=nx, ny=ny, nz=nz), moist=moist)
+    f = {"pressure": c.pressure, "th": c.species["theta"], "pii": c.exner, "rho": c.density, "qv": c.species["qv"],
+         "qc": c.species["qc"], "qr": c.species["qr"], "qs": c.species["qs"], "dz": c.dz_mass}
+    return c, f
+
+
+def test_mp_simple_conserves_water(oracle_lib):
+    """Every conversion moves water between qv, qc, qr and qs, and
+    sedimentation moves it down or out into the accumulated precipitation:
+    sum(q*rho*dz) over the tile plus the precipitation is conserved to
+    round-off over several calls."""
+    O = oracle_lib
+    c, f = _mp_inputs()
+    hs = 2
+
+    def water(d):
+        return float(sum((d[k].astype(np.float64) * f["rho"] * f["dz"])[hs:-hs, :, hs:-hs].sum()
+                         for k in ("qv", "qc", "qr", "qs")))
+    w0 = water(f)
+    cur = dict(f)
+    rain = snow = None
+    for _ in range(4):
+        out = O.mp_simple(cur, 20.0, hs, rain, snow)
+        assert not out["stop"]
+        cur = dict(cur, **{k: out[k] for k in ("th", "qv", "qc", "qr", "qs")})
+        rain, snow = out["acc_rain"], out["acc_snow"]
+    assert abs(water(cur) + rain.sum() - w0) / w0 < 1e-6
+    assert rain.sum() > 0 and (snow <= rain + 1e-12).all()   # snowfall is counted in both
+    # columns outside the tile are untouched
+    assert np.array_equal(cur["qv"][:hs], f["qv"][:hs]) and not rain[:hs].any()
+
+
+def test_mp_simple_latent_heating(oracle_lib):
+    """Condensation warms and evaporation cools: where qv + qc grew into
+    cloud the potential temperature rose, where cloud evaporated it fell."""
+    O = oracle_lib
+    c, f = _mp_inputs(moist=2.0)
+    out = O.mp_simple(f, 20.0, 2)
+    dqv = out["qv"].astype(np.float64) - f["qv"]
+    dth = out["th"].astype(np.float64) - f["th"]
+    cond = dqv < -1e-6
+    assert cond.any() and (dth[cond] > 0).all()
+
+
+def test_mp_simple_f32_tracks_f64(oracle_lib):
+    O = oracle_lib
+    c, f = _mp_inputs(seed=5, nx=30, ny=28, nz=15)
+    a = O.mp_simple(f, 20.0, 2)
+    b = O.mp_simple(f, 20.0, 2, dtype=np.float64)
+    for k in ("th", "qv"):
+        rel = np.abs(a[k].astype(np.float64) - b[k]) / np.maximum(np.abs(b[k]), 1e-6 * np.abs(b[k]).max())
+        assert rel.max() < 1e-4, k
