@@ -84,6 +84,8 @@ _METRIC_FIELDS = {
     "advection_dz": L.F_ADVECTION_DZ,
     # read only by the simple microphysics (mp)
     "pressure": L.F_PRESSURE, "exner": L.F_EXNER, "dz_mass": L.F_DZ_MASS,
+    # kept on the device for restarts only
+    "dz_interface": L.F_DZ_INTERFACE,
 }
 
 
@@ -102,7 +104,7 @@ class Domain:
         self.north_boundary, self.south_boundary, self.east_boundary, self.west_boundary = boundaries
         self.u = self.v = self.w = self.density = None
         self.jacobian = self.jacobian_u = self.jacobian_v = self.jacobian_w = self.advection_dz = None
-        self.pressure = self.exner = self.dz_mass = None
+        self.pressure = self.exner = self.dz_mass = self.dz_interface = None
         self.adv_vars: dict[str, np.ndarray] = {}
         self.forcing: dict[str, tuple[np.ndarray, np.ndarray | None]] = {}
         self._h = None
@@ -214,6 +216,52 @@ class Domain:
             self.adv_vars[name] = a
         return a
 
+    def _shape_of(self, name: str) -> tuple[int, int, int]:
+        if name == "u":
+            return (self.ny, self.nz, self.nx + 1)
+        if name == "v":
+            return (self.ny + 1, self.nz, self.nx)
+        return (self.ny, self.nz, self.nx)
+
+    def download(self, names) -> dict[str, np.ndarray]:
+        """Copy several resident fields to new host arrays with one wait on
+        the device (icar_adv_download); species are also stored back into
+        adv_vars."""
+        names = list(names)
+        ids = (C.c_int32 * max(len(names), 1))(*[self._field_id(n) for n in names])
+        out = {n: np.empty(self._shape_of(n), np.float32) for n in names}
+        ptrs = (C.c_void_p * max(len(names), 1))(*[out[n].ctypes.data for n in names])
+        L.check(L.load().icar_adv_download(self.handle, len(names), ids, ptrs), self.handle)
+        for n in names:
+            if n in self.adv_vars:
+                self.adv_vars[n] = out[n]
+        return out
+
+    def upload_many(self, arrays: dict) -> None:
+        """Write several fields from host arrays (icar_adv_upload)."""
+        names = list(arrays)
+        keep = [np.ascontiguousarray(arrays[n], np.float32) for n in names]
+        for n, a in zip(names, keep):
+            if a.size != int(np.prod(self._shape_of(n))):
+                raise ValueError(f"{n}: expected {self._shape_of(n)} values, got {a.shape}")
+        ids = (C.c_int32 * max(len(names), 1))(*[self._field_id(n) for n in names])
+        ptrs = (C.c_void_p * max(len(names), 1))(*[a.ctypes.data for a in keep])
+        L.check(L.load().icar_adv_upload(self.handle, len(names), ids, ptrs), self.handle)
+
+    def restart_vars(self) -> list[str]:
+        """The fields options%restart_vars lists for advection
+        (adv_std_var_request, advect.f90:95-107)."""
+        return restart_vars(self._options)
+
+    def download_restart(self) -> dict[str, np.ndarray]:
+        """The advection restart set (u, v, w, dz_interface, qv) in one
+        bulk download."""
+        return self.download(self.restart_vars())
+
+    def restore_restart(self, arrays: dict) -> None:
+        """Write a restart set back (icar_adv_upload)."""
+        self.upload_many(arrays)
+
     def relax_filter(self) -> np.ndarray:
         out = np.zeros((self.ny, self.nx), np.float32)
         L.check(L.load().icar_adv_get_field(self.handle, L.F_RELAX_FILTER, L.f32_ptr(out), None), self.handle)
@@ -290,6 +338,20 @@ def adv_var_request(options: Options) -> None:
     for i in range(nv.value):
         if int(adv[i]) not in options.vars_to_advect:
             options.vars_to_advect.append(int(adv[i]))
+
+
+def restart_vars(options: Options) -> list[str]:
+    """Names of the fields options%restart_vars lists for advection, in the
+    reference's order (adv_std_var_request, advect.f90:95-107)."""
+    n = C.c_int32(8)
+    ids = (C.c_int32 * 8)()
+    opts = options.to_c()
+    L.check(L.load().icar_adv_restart_vars(C.byref(opts), ids, C.byref(n)))
+    names = []
+    for i in range(n.value):
+        fid = int(ids[i])
+        names.append(next((k for k, v in _METRIC_FIELDS.items() if v == fid), None) or L.SPECIES_NAMES[fid])
+    return names
 
 
 def adv_init(domain: Domain, options: Options) -> None:

@@ -70,6 +70,8 @@ struct icar_adv_domain {
     // snow accumulations (nx*ny each) and the device stop flag
     DevBuf pressure, exner, dz_mass;
     bool have_pressure = false, have_exner = false, have_dz_mass = false;
+    DevBuf dz_interface;                      // kept for restarts only (the path does not read it)
+    bool have_dz_interface = false;
     double *acc_precip = nullptr;             // rain [0, nx*ny), snow [nx*ny, 2*nx*ny)
     int *mp_stop = nullptr;
     bool mp_ran = false;
@@ -324,6 +326,12 @@ int resolve(icar_adv_t *h, int field, FieldRef &r)
     case ICAR_F_JACOBIAN_W: r = {&h->jac_w, nx, ny, nz, &h->have_jac_w}; return ICAR_ADV_OK;
     case ICAR_F_ADVECTION_DZ: r = {&h->dz, nx, ny, nz, &h->have_dz}; return ICAR_ADV_OK;
     case ICAR_F_RELAX_FILTER: r = FieldRef{}; r.ex = nx; r.ey = ny; r.ez = 1; r.is_filter = true; return ICAR_ADV_OK;
+    case ICAR_F_DZ_INTERFACE: {
+        int e = alloc(h, h->dz_interface, h->n_cell);
+        if (e) return e;
+        r = {&h->dz_interface, nx, ny, nz, &h->have_dz_interface};
+        return ICAR_ADV_OK;
+    }
     case ICAR_F_PRESSURE: case ICAR_F_EXNER: case ICAR_F_DZ_MASS: {
         DevBuf *b = field == ICAR_F_PRESSURE ? &h->pressure : field == ICAR_F_EXNER ? &h->exner : &h->dz_mass;
         bool *f = field == ICAR_F_PRESSURE ? &h->have_pressure : field == ICAR_F_EXNER ? &h->have_exner : &h->have_dz_mass;
@@ -349,7 +357,7 @@ int resolve(icar_adv_t *h, int field, FieldRef &r)
     return ICAR_ADV_OK;
 }
 
-int copy_field(icar_adv_t *h, int field, float *host, const int64_t *strides, bool to_device)
+int copy_field(icar_adv_t *h, int field, float *host, const int64_t *strides, bool to_device, bool wait = true)
 {
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
     if (!host) return fail(h, ICAR_ADV_BAD_ARG, "host pointer is NULL");
@@ -424,7 +432,7 @@ int copy_field(icar_adv_t *h, int field, float *host, const int64_t *strides, bo
     if (to_device) {
         if (r.flag) *r.flag = true;
         if (r.species >= 0 && !r.is_forcing && !r.is_dqdt) h->have_q[r.species] = true;
-    } else {
+    } else if (wait) {
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     }
     return ICAR_ADV_OK;
@@ -830,7 +838,7 @@ int icar_adv_destroy(icar_adv_t *h)
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
                       &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
                       &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp, &h->Gc,
-                      &h->DJR, &h->Wp, &h->dtbuf, &h->pressure, &h->exner, &h->dz_mass})
+                      &h->DJR, &h->Wp, &h->dtbuf, &h->pressure, &h->exner, &h->dz_mass, &h->dz_interface})
         release(*b);
     if (h->acc_precip) cudaFree(h->acc_precip);
     if (h->mp_stop) cudaFree(h->mp_stop);
@@ -863,6 +871,45 @@ int icar_adv_get_field(icar_adv_t *h, int32_t field, float *host, const int64_t 
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
     cudaSetDevice(h->desc.device);
     return copy_field(h, field, host, strides, false);
+}
+
+int icar_adv_restart_vars(const icar_adv_opts *opts, int32_t *vars, int32_t *n)
+{
+    // adv_std_var_request, src/physics/advect.f90:95-107: the same set for
+    // both schemes (advection_driver.f90:46-56)
+    (void)opts;
+    if (!n) return fail(nullptr, ICAR_ADV_BAD_ARG, "n is NULL");
+    const int32_t set[5] = {ICAR_F_U, ICAR_F_V, ICAR_F_W, ICAR_F_DZ_INTERFACE, ICAR_F_QV};
+    if (vars) {
+        if (*n < 5) return fail(nullptr, ICAR_ADV_BAD_ARG, "vars needs room for 5 ids");
+        memcpy(vars, set, sizeof(set));
+    }
+    *n = 5;
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_download(icar_adv_t *h, int32_t n, const int32_t *fields, float *const *host)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (n < 0 || (n > 0 && (!fields || !host))) return fail(h, ICAR_ADV_BAD_ARG, "bad field list");
+    cudaSetDevice(h->desc.device);
+    for (int f = 0; f < n; f++) {
+        int e = copy_field(h, fields[f], host[f], nullptr, false, false);
+        if (e) return e;
+    }
+    return icar_adv_sync(h);
+}
+
+int icar_adv_upload(icar_adv_t *h, int32_t n, const int32_t *fields, const float *const *host)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (n < 0 || (n > 0 && (!fields || !host))) return fail(h, ICAR_ADV_BAD_ARG, "bad field list");
+    cudaSetDevice(h->desc.device);
+    for (int f = 0; f < n; f++) {
+        int e = copy_field(h, fields[f], const_cast<float *>(host[f]), nullptr, true);
+        if (e) return e;
+    }
+    return icar_adv_sync(h);
 }
 
 static int device_copy(icar_adv_t *h, int32_t field, float *dev, bool to_handle)

@@ -154,6 +154,19 @@ int icar_adv_destroy(icar_adv_t *h);
 int icar_adv_set_field(icar_adv_t *h, int32_t field, const float *host, const int64_t *strides);
 int icar_adv_get_field(icar_adv_t *h, int32_t field, float *host, const int64_t *strides);
 
+/* Restarts.  icar_adv_restart_vars gives the field ids the reference lists
+ * for advection restarts (options%restart_vars in adv_std_var_request,
+ * src/physics/advect.f90:95-107, the same for both schemes): u, v, w,
+ * dz_interface, water_vapor; vars may be NULL to ask for the count.
+ * icar_adv_download copies n resident fields to host arrays (contiguous
+ * Fortran order) with one wait at the end instead of one per field, and
+ * icar_adv_upload writes them back -- every species and forcing field, the
+ * winds and metric terms, pressure/exner/dz and dz_interface (which the
+ * handle keeps only for restarts). */
+int icar_adv_restart_vars(const icar_adv_opts *opts, int32_t *vars, int32_t *n);
+int icar_adv_download(icar_adv_t *h, int32_t n, const int32_t *fields, float *const *host);
+int icar_adv_upload(icar_adv_t *h, int32_t n, const int32_t *fields, const float *const *host);
+
 /* Same with device memory on the handle's device (contiguous Fortran order).
  * Ordered on the handle's stream. */
 int icar_adv_set_field_device(icar_adv_t *h, int32_t field, const float *dev);

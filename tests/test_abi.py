@@ -78,3 +78,21 @@ def test_null_handle_is_an_error_not_a_crash(cuda_lib):
     assert lib.icar_adv_advect(None, C.c_float(1.0)) == cuda_lib.BAD_ARG
     assert lib.icar_adv_sync(None) == cuda_lib.BAD_ARG
     assert lib.icar_adv_destroy(None) == 0
+
+
+def test_restart_vars_match_reference_request(cuda_lib):
+    """adv_std_var_request (advect.f90:95-107) asks for u, v, w,
+    dz_interface and water_vapor as restart variables, for both schemes."""
+    from hicar_b200 import Options, kADV_STD, restart_vars
+    lib = cuda_lib.load()
+    assert restart_vars(Options()) == ["u", "v", "w", "dz_interface", "qv"]
+    o = Options()
+    o.adv_options.advection = kADV_STD
+    assert restart_vars(o) == ["u", "v", "w", "dz_interface", "qv"]
+    n = C.c_int32(0)
+    assert lib.icar_adv_restart_vars(None, None, C.byref(n)) == 0 and n.value == 5
+    ids = (C.c_int32 * 4)()
+    n = C.c_int32(4)
+    assert lib.icar_adv_restart_vars(None, ids, C.byref(n)) == cuda_lib.BAD_ARG
+    assert lib.icar_adv_download(None, 0, None, None) == cuda_lib.BAD_ARG
+    assert lib.icar_adv_upload(None, 0, None, None) == cuda_lib.BAD_ARG
