@@ -44,7 +44,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="full_species",
-                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large", "wind", "mp"])
+                   choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large", "wind", "mp",
+                            "std"])
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-duration", type=float, default=6.0)
     p.add_argument("--serve-steps-scale", type=float, default=0.1)
@@ -122,15 +123,17 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- CPU oracle
-def cpu_rate(case, threads: int, target_s: float = 10.0, max_steps: int = 200) -> tuple[float, float, int]:
+def cpu_rate(case, threads: int, target_s: float = 10.0, max_steps: int = 200,
+             scheme: dict | None = None) -> tuple[float, float, int]:
     """Cell-species updates/s of the oracle (C restatement, OpenMP) on case:
     whole steps until about target_s seconds of CPU work (at least 2).
+    scheme: make_opts keywords (default MPDATA order 2 + FCT).
     Returns (rate, seconds, steps)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from hicar_b200.build import build_oracle
     build_oracle()
     from oracle import oracle as O
-    opts = O.make_opts()
+    opts = O.make_opts(**(scheme or {}))
     O.advect(case, opts, case.dt)  # warm (page-in, thread pool)
     t0 = time.perf_counter()
     c, steps = case, 0
@@ -562,6 +565,95 @@ def run_mp(args):
         "advect_then_mp_ms": ms_pair, "clocks": clk}), flush=True)
 
 
+# ------------------------------------------------------------ standard scheme
+STD_SCHEME = {"advection": 1, "h_order": 5, "v_order": 3, "flux_corr": 1, "rk3": 1}
+
+
+def run_std(args):
+    """The standard scheme in HICAR's default setting (RK3, 5th-order
+    horizontal and 3rd-order vertical fluxes, WRF monotonic flux
+    correction) on the full-species domain: the fused kernels and the
+    one-kernel-per-stage path, each timed with CUDA events on the library's
+    stream, against the HBM roofline of the step's bytes; the oracle on a
+    y-slab of the same domain as the CPU baseline."""
+    import torch
+    from hicar_b200 import _lib as L, replicas as R, roofline
+    from hicar_b200.advection import AdvOptions, Domain, Options, PhysicsOptions, TimeOptions, adv_init
+
+    if not R.from_env().is_root:
+        return
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    case, desc = make_case("full_species", 100)
+    opts = Options(physics=PhysicsOptions(advection=1),
+                   adv_options=AdvOptions(h_order=5, v_order=3, flux_corr=1), time_options=TimeOptions(RK3=True))
+    S = len(case.species)
+    lib = L.load()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    def timed(staged: bool, steps: int):
+        d = Domain.from_case(case, device=local)
+        adv_init(d, opts)
+        if staged:
+            d.use_staged_kernels(True)
+        h = d.handle
+        L.check(lib.icar_adv_set_stream(h, C.c_void_p(stream.cuda_stream)), h)
+        for _ in range(args.warmup):
+            L.check(lib.icar_adv_advect(h, C.c_float(case.dt)), h)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            L.check(lib.icar_adv_advect(h, C.c_float(case.dt)), h)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        # launch count of one more (profiled) round of steps
+        L.check(lib.icar_adv_profile(h, 1), h)
+        for _ in range(steps):
+            L.check(lib.icar_adv_advect(h, C.c_float(case.dt)), h)
+        kms, kl, alll, passes = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
+        L.check(lib.icar_adv_profile_read(h, C.byref(kms), C.byref(kl), C.byref(alll), C.byref(passes)), h)
+        L.check(lib.icar_adv_profile(h, 0), h)
+        d.close()
+        return ms, alll.value / steps
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.4)
+    ms_fused, l_fused = timed(False, args.steps)
+    ms_staged, l_staged = timed(True, max(3, args.steps // 4))
+    clk = clocks.stop()
+    cs = case.cells() * S
+    peak, kind = roofline.hbm_peak()
+    # three stages: q -> t1 (8 B), (t1, q) -> t2 (12 B), (t2, q) -> q (12 B) per cell-species;
+    # per cell: prep reads 9 fields and writes 5 (56 B), each stage reads U_m, V_m, W_m, G, DJR (60 B)
+    step_bytes = cs * 32.0 + case.cells() * 116.0
+    line = {
+        "metric": "standard-scheme cell-species updates/s", "value": cs / (ms_fused / 1e3),
+        "unit": "cell-species updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_fused, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "standard scheme (RK3, h_order 5, v_order 3, WRF monotonic flux correction) on the "
+                               + desc},
+        "roofline": {"kernel": "k_std_prep + 3 x (k_std_ring + k_std_fused) per advect call", "bound": "hbm",
+                     "achieved": step_bytes / (ms_fused / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": step_bytes / (ms_fused / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": kind,
+                     "algorithmic_bytes_per_launch": step_bytes,
+                     "bytes_model": "32 B per cell-species (three RK3 stages) + 116 B per cell (prep, and the "
+                                    "Courant and metric fields once per stage)"},
+        "staged": {"ms_per_step": ms_staged, "value": cs / (ms_staged / 1e3), "launches_per_step": l_staged},
+        "speedup_vs_staged": ms_staged / ms_fused, "gpu_launches_per_step": l_fused, "clocks": clk}
+    if not args.no_cpu_baseline:
+        threads = len(os.sched_getaffinity(0))
+        sample = cpu_sample(case, 16)
+        rate, el, nst = cpu_rate(sample, threads, scheme=STD_SCHEME)
+        line["cpu_baseline"] = {"value": rate, "unit": "cell-species updates/s", "cores": threads, "kind": "port",
+                                "sample": f"512x16x40 slab of the workload, 12 fields, {nst} steps, {el:.1f} s "
+                                          "(C restatement, OpenMP)"}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------ ensemble
 ENSEMBLE_DESC = ("batched uneven ensemble: 64 independent domains, nx,ny ~ U[64,384], nz ~ U[20,50], "
                  "12 fields each, dt 20 s, one graph launch per step vs 64 plain launches")
@@ -787,6 +879,8 @@ def main():
         run_wind(args)
     elif args.workload == "mp":
         run_mp(args)
+    elif args.workload == "std":
+        run_std(args)
     else:
         run_b200(args)
 

@@ -22,6 +22,7 @@
 #include "mpdata_fused.cuh"
 #include "mpdata_kernels.cuh"
 #include "std_kernels.cuh"
+#include "std_fused.cuh"
 #include "batch_kernels.cuh"
 #include "wind_kernels.cuh"
 #include "mp_kernels.cuh"
@@ -77,8 +78,10 @@ struct icar_adv_domain {
     bool mp_ran = false;
     std::vector<DevBuf> qn, q1s;               // fused path: next state and pass-1 result per species
     bool fused_ready = false;
+    bool std_ready = false;      // fused standard-scheme buffers and kernel attributes
+    bool std_staged_ready = false;
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
-    int path = 0;      // 0 = fused MPDATA kernel when eligible, 1 = staged kernels
+    int path = 0;      // 0 = fused kernels (MPDATA order 2, every standard-scheme setting), 1 = staged kernels
     int mp_shape = 1;  // tile shape of the fused correction kernel (icar::mp_shape_ty)
     int sp_group = 0;  // species per thread of the fused upwind pass (0 = all)
     // diagnostics: launch counter and optional event timing of the species kernels
@@ -188,7 +191,7 @@ int64_t footprint_bytes(const icar_adv_desc &d, const icar_adv_opts &o)
     else if (o.advection == ICAR_ADV_MPDATA)
         total += f * (int64_t)(nc + 2 * (nu + nv + nc));               // staged scratch
     else
-        total += f * (int64_t)(2 * (nu + nv + nzf) + 4 * nc);
+        total += f * (int64_t)nc * (2 * d.n_species + 2);              // fused: two stage results per species, G, DJR
     total += f * (int64_t)d.nx * d.ny + 4 * (int64_t)d.nx * d.ny;
     return total;
 }
@@ -545,6 +548,25 @@ int mpdata_staged(icar_adv_t *h, int s)
 
 // One adv_std_advect3d call: fluxes from qf scaled by t_factor, optional WRF
 // correction against qold, update written to qout (may alias qold).
+// Scratch of the staged standard scheme (flux arrays, RK3 temporary, WRF
+// work arrays), allocated on first use.
+int ensure_std_staged(icar_adv_t *h)
+{
+    if (h->std_staged_ready) return ICAR_ADV_OK;
+    const size_t nc = h->n_cell, nu = h->n_u, nv = h->n_v;
+    int e;
+    if ((e = alloc(h, h->fx, nu)) || (e = alloc(h, h->fy, nv)) || (e = alloc(h, h->fz, h->n_zf)) ||
+        (e = alloc(h, h->temp, nc)))
+        return e;
+    if (h->opts.flux_corr == 1)
+        if ((e = alloc(h, h->ufx, nu)) || (e = alloc(h, h->ufy, nv)) || (e = alloc(h, h->ufz, h->n_zf)) ||
+            (e = alloc(h, h->dq, nc)) || (e = alloc(h, h->sin_, nc)) || (e = alloc(h, h->sout, nc)))
+            return e;
+    h->std_staged_ready = true;
+    return ICAR_ADV_OK;
+}
+
+// Callers run ensure_std_staged first (qout may be the scratch temp array).
 int std_advect3d(icar_adv_t *h, const float *qf, const float *qold, float *qout, float t_factor, int flux_corr)
 {
     const Geo &g = h->g;
@@ -644,13 +666,92 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
     return ICAR_ADV_OK;
 }
 
+// Fused standard scheme: prep (Courant fluxes, G, DJR) then one launch per
+// adv_std_advect3d call for all species (three with RK3), results in
+// per-species buffers swapped into place.
+int ensure_std_fused(icar_adv_t *h)
+{
+    const int S = h->desc.n_species;
+    int e;
+    if (!h->std_ready) {
+        h->qn.resize(S);
+        h->q1s.resize(S);
+        if ((e = alloc(h, h->Gc, h->n_cell)) || (e = alloc(h, h->DJR, h->n_cell))) return e;
+        for (int s = 0; s < S; s++)
+            if ((e = alloc(h, h->qn[s], h->n_cell)) || (e = alloc(h, h->q1s[s], h->n_cell))) return e;
+        cudaError_t ce = icar::std_fused_setup();
+        if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaFuncSetAttribute: %s", cudaGetErrorString(ce));
+        h->std_ready = true;
+    }
+    return ICAR_ADV_OK;
+}
+
+int std_fused_step(icar_adv_t *h, float dt)
+{
+    const Geo &g = h->g;
+    const int S = h->desc.n_species;
+    int e = ensure_std_fused(h);
+    if (e) return e;
+    const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
+    const float *rho = h->have_rho ? h->rho.p : h->jac.p;  // only read when advect_density
+    icar::k_std_prep<<<blocks_for(nf, 256), 256, 0, h->stream>>>(
+        g, h->desc.dx, dt, h->opts.advect_density, h->u.p, h->v.p, h->w.p, rho, h->jac.p, h->jac_u.p, h->jac_v.p,
+        h->jac_w.p, h->dz.p, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p, h->DJR.p);
+    if (h->opts.debug &&
+        icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p,
+                            h->opts.advect_density))
+        return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
+    const int ho = h->opts.h_order, vo = h->opts.v_order, hs = h->hs;
+    const bool corr = h->opts.flux_corr == 1;
+    auto stage = [&](std::vector<DevBuf> *qf, std::vector<DevBuf> *out, float tf, bool c) {
+        icar::SpeciesPtrs sp{};
+        for (int s = 0; s < S; s++) {
+            sp.q0[s] = h->q[s].p;
+            sp.q1[s] = (qf ? *qf : h->q)[s].p;
+            sp.out[s] = (*out)[s].p;
+        }
+        return icar::std_fused_launch(h->stream, c, ho, vo, g, hs, tf, sp, S, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p,
+                                      h->DJR.p);
+    };
+    cudaEvent_t c0 = nullptr, c1 = nullptr;
+    if (h->profiling && S > 0) {
+        cudaEventCreate(&c0);
+        cudaEventCreate(&c1);
+        cudaEventRecord(c0, h->stream);
+    }
+    int bad = 0, nl = 1;
+    if (S > 0) {
+        if (h->opts.rk3) {
+            // advection_driver.f90:100-110: q + 1/3, q + 1/2 from the first
+            // result, then the full step (with the flux correction) from the second
+            bad |= stage(nullptr, &h->q1s, 0.333f, false);
+            bad |= stage(&h->q1s, &h->qn, 0.5f, false);
+            bad |= stage(&h->qn, &h->q1s, 1.0f, corr);
+            nl += 6;
+        } else {
+            bad |= stage(nullptr, &h->qn, 1.0f, corr);
+            nl += 2;
+        }
+    }
+    if (h->profiling && S > 0) {
+        cudaEventRecord(c1, h->stream);
+        h->corr_events.emplace_back(c0, c1);
+    }
+    if (bad) return fail(h, ICAR_ADV_BAD_ARG, "h_order and v_order must be 1, 3 or 5");
+    e = check_launch(h, "fused standard-scheme kernels", nl);
+    if (e) return e;
+    for (int s = 0; s < S; s++) std::swap(h->q[s], h->opts.rk3 ? h->q1s[s] : h->qn[s]);
+    return ICAR_ADV_OK;
+}
+
 int advect_impl(icar_adv_t *h, float dt)
 {
     int e = ensure_ready(h);
     if (e) return e;
     if (!(dt >= 0.0f) || !std::isfinite(dt)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite and >= 0");
     const bool mp = h->opts.advection == ICAR_ADV_MPDATA;
-    if (mp && !h->opts.rk3 && h->path == 0 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct)) {
+    const bool fused_mp = mp && !h->opts.rk3 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct);
+    if (h->path == 0 && (fused_mp || !mp)) {
         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
         int64_t before = h->launches;
         if (h->profiling) {
@@ -658,7 +759,7 @@ int advect_impl(icar_adv_t *h, float dt)
             cudaEventCreate(&ev1);
             cudaEventRecord(ev0, h->stream);
         }
-        e = mpdata_fused_step(h, dt);
+        e = mp ? mpdata_fused_step(h, dt) : std_fused_step(h, dt);
         if (e) return e;
         if (h->profiling) {
             cudaEventRecord(ev1, h->stream);
@@ -676,6 +777,7 @@ int advect_impl(icar_adv_t *h, float dt)
     }
     e = compute_wind(h, dt);
     if (e) return e;
+    if (!mp && (e = ensure_std_staged(h))) return e;
     if (h->opts.debug) {
         e = icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p,
                                 h->opts.advect_density || mp);
@@ -804,17 +906,8 @@ int icar_adv_create(const icar_adv_desc *desc, const icar_adv_opts *opts, icar_a
         return bail(e);
     for (int s = 0; s < S; s++)
         if ((e = alloc(h, h->q[s], nc))) return bail(e);
-    if (opts->advection == ICAR_ADV_MPDATA) {
-        // the staged MPDATA scratch is allocated on first use (mpdata_staged)
-    } else {
-        if ((e = alloc(h, h->fx, nu)) || (e = alloc(h, h->fy, nv)) || (e = alloc(h, h->fz, h->n_zf)) ||
-            (e = alloc(h, h->temp, nc)))
-            return bail(e);
-        if (opts->flux_corr == 1)
-            if ((e = alloc(h, h->ufx, nu)) || (e = alloc(h, h->ufy, nv)) || (e = alloc(h, h->ufz, h->n_zf)) ||
-                (e = alloc(h, h->dq, nc)) || (e = alloc(h, h->sin_, nc)) || (e = alloc(h, h->sout, nc)))
-                return bail(e);
-    }
+    // the scratch of either scheme is allocated on first use (ensure_fused,
+    // ensure_std_fused, mpdata_staged, std_advect3d)
     relax_filter(desc->nx, desc->ny, h->hs, desc->north_boundary, desc->south_boundary, desc->east_boundary,
                  desc->west_boundary, h->filter_host);
     if ((e = upload_filter(h))) return bail(e);
