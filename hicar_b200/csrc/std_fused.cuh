@@ -216,12 +216,12 @@ __device__ __forceinline__ float std_zflux(int f, int nz, const float *Q, float 
     float F;
     if (VORD == 3 || f == 2 || f == nz - 2) {
         F = 7.0f * (Q[3] + Q[2]) - (Q[4] + Q[1]);
-        F = (ww * F) / 12.0f;
-        F = F - (fabsf(ww) / 12.0f) * (3.0f * (Q[3] - Q[2]) - (Q[4] - Q[1]));
+        F = div12(ww * F);
+        F = F - div12(fabsf(ww)) * (3.0f * (Q[3] - Q[2]) - (Q[4] - Q[1]));
     } else {
         F = 37.0f * (Q[3] + Q[2]) - 8.0f * (Q[4] + Q[1]) + (Q[5] + Q[0]);
-        F = (ww * F) / 60.0f;
-        F = F - (fabsf(ww) / 60.0f) * (10.0f * (Q[3] - Q[2]) - 5.0f * (Q[4] - Q[1]) + (Q[5] - Q[0]));
+        F = div60(ww * F);
+        F = F - div60(fabsf(ww)) * (10.0f * (Q[3] - Q[2]) - 5.0f * (Q[4] - Q[1]) + (Q[5] - Q[0]));
     }
     return F;
 }
@@ -628,7 +628,7 @@ __device__ __forceinline__ void std_corr_tile(float *sm, const Geo &g, int its, 
 // Grid: blockIdx.x = tile * S + species (the species of a tile on
 // consecutive CTAs share its Courant and metric planes through L2).
 template <int HORD, int VORD, class SH>
-__global__ void __launch_bounds__(SH::NT, SH::CORR ? 2 : 3)
+__global__ void __launch_bounds__(SH::NT, SH::CORR ? 1 : 3)
     k_std_fused(Geo g, int its, int ite, int jts, int jte, float tf, const __grid_constant__ SpeciesPtrs sp,
                 int nspecies, int tiles_x, const float *__restrict__ Um, const float *__restrict__ Vm,
                 const float *__restrict__ Wm, const float *__restrict__ Gc, const float *__restrict__ DJR)
@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(SH::NT, SH::CORR ? 2 : 3)
 }
 
 using StdStageShape = stdf::Shape<16, 8, false>;
-using StdCorrShape = stdf::Shape<12, 8, true>;
+using StdCorrShape = stdf::Shape<28, 32, true>;
 
 template <int HORD, int VORD>
 inline cudaError_t std_fused_attr()

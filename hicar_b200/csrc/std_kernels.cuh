@@ -8,8 +8,14 @@
 // level 0 the ground (always 0) and level nz the model top.
 #pragma once
 #include "common.cuh"
+#include "const_div.h"
 
 namespace icar {
+
+// x/12 and x/60 of the flux formulas, correctly rounded, as one double
+// product (const_div.h): branch-free, unlike the general division.
+__device__ __forceinline__ float div12(float x) { return __double2float_rn(__dmul_rn((double)x, ICAR_RCP12_D)); }
+__device__ __forceinline__ float div60(float x) { return __double2float_rn(__dmul_rn((double)x, ICAR_RCP60_D)); }
 
 __device__ __forceinline__ size_t izf(const Geo &g, int i, int k, int j)
 {
@@ -87,12 +93,12 @@ __device__ __forceinline__ float hflux(int hord, const float *r, size_t s, float
         F = flux1(R(-1), R(0), uu);
     } else if (hord == 3) {
         F = 7.0f * (R(0) + R(-1)) - (R(1) + R(-2));
-        F = (uu * F) / 12.0f;
-        F = F - (fabsf(uu) / 12.0f) * (3.0f * (R(0) - R(-1)) - (R(1) - R(-2)));
+        F = div12(uu * F);
+        F = F - div12(fabsf(uu)) * (3.0f * (R(0) - R(-1)) - (R(1) - R(-2)));
     } else {
         F = 37.0f * (R(0) + R(-1)) - 8.0f * (R(1) + R(-2)) + (R(2) + R(-3));
-        F = (uu * F) / 60.0f;
-        F = F - (fabsf(uu) / 60.0f) * (10.0f * (R(0) - R(-1)) - 5.0f * (R(1) - R(-2)) + (R(2) - R(-3)));
+        F = div60(uu * F);
+        F = F - div60(fabsf(uu)) * (10.0f * (R(0) - R(-1)) - 5.0f * (R(1) - R(-2)) + (R(2) - R(-3)));
     }
 #undef R
     return F;
@@ -135,12 +141,12 @@ __global__ void k_flux3(Geo g, int hord, int vord, int is, int ie, int js, int j
                 F = flux1(QZ(k - 1), QZ(k), ww);
             } else if (vord == 3 || k == 2 || k == nz - 2) {
                 F = 7.0f * (QZ(k) + QZ(k - 1)) - (QZ(k + 1) + QZ(k - 2));
-                F = (ww * F) / 12.0f;
-                F = F - (fabsf(ww) / 12.0f) * (3.0f * (QZ(k) - QZ(k - 1)) - (QZ(k + 1) - QZ(k - 2)));
+                F = div12(ww * F);
+                F = F - div12(fabsf(ww)) * (3.0f * (QZ(k) - QZ(k - 1)) - (QZ(k + 1) - QZ(k - 2)));
             } else {
                 F = 37.0f * (QZ(k) + QZ(k - 1)) - 8.0f * (QZ(k + 1) + QZ(k - 2)) + (QZ(k + 2) + QZ(k - 3));
-                F = (ww * F) / 60.0f;
-                F = F - (fabsf(ww) / 60.0f) *
+                F = div60(ww * F);
+                F = F - div60(fabsf(ww)) *
                             (10.0f * (QZ(k) - QZ(k - 1)) - 5.0f * (QZ(k + 1) - QZ(k - 2)) + (QZ(k + 2) - QZ(k - 3)));
             }
             fz[zf] = F;
