@@ -149,7 +149,7 @@ __global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *_
 
 // Persistent correction kernel: items are (member, species, i0, j0).
 template <bool FCT, class SH>
-__global__ void __launch_bounds__(SH::NT, (SH::NT <= 128 ? 5 : 3))
+__global__ void __launch_bounds__(SH::NT, (SH::NT <= 128 ? 5 : SH::NT <= 256 ? 3 : SH::NT <= 512 ? 2 : 1))
     k_batch_corr(const BatchMember *__restrict__ mem, const int4 *__restrict__ items, int n_items,
                  int *__restrict__ counter)
 {

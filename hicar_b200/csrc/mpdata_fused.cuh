@@ -305,7 +305,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
     pl.load(P(S_G + 1), Gc, 1, false);
     cp_async_commit();
 
-    // per-output-cell z state (two output rows per warp)
+    // per-output-cell z state (RPW output rows per warp)
     // r_q1dn / r_q0dn: q1 and q0 one level below the level being limited;
     // r_q1dd: q1 two levels below (the level under the corrective pass).
     float r_fz[RPW], r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_w2l[RPW], r_q1dn[RPW], r_q0dn[RPW], r_q1dd[RPW];
@@ -630,7 +630,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
 }
 
 template <bool FCT, class SH>
-__global__ void __launch_bounds__(SH::NT, (SH::NT <= 128 ? 5 : 3))
+__global__ void __launch_bounds__(SH::NT, (SH::NT <= 128 ? 5 : SH::NT <= 256 ? 3 : SH::NT <= 512 ? 2 : 1))
     k_mp_corr(Geo g, SpeciesPtrs sp, int nspecies, int tiles_x, const float *__restrict__ Um,
               const float *__restrict__ Vm, const float *__restrict__ Wp, const float *__restrict__ Gc,
               const float *__restrict__ DJR, const float *__restrict__ dz)
@@ -694,9 +694,9 @@ namespace icar {
 // Tile shapes of the fused correction kernel (selected per grid shape by
 // the autotuner): output rows per tile and warps per CTA.
 using MpShape8 = mpf::Shape<8, 4>;
-using MpShape16 = mpf::Shape<16, 8>;
+using MpShape16 = mpf::Shape<16, 16>;
 using MpShape24 = mpf::Shape<24, 8>;
-using MpShape32 = mpf::Shape<32, 8>;
+using MpShape32 = mpf::Shape<32, 32>;
 constexpr int MP_NSHAPES = 4;
 inline int mp_shape_ty(int shape)
 {
