@@ -103,6 +103,7 @@ _PROTOS = {
     "icar_adv_mp_simple": (C.c_int, [C.c_void_p, C.c_float]),
     "icar_adv_get_precipitation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "icar_adv_set_precipitation": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "icar_adv_step_host": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "icar_adv_restart_vars": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "icar_adv_download": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_void_p)]),
     "icar_adv_upload": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_void_p)]),

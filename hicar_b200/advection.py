@@ -436,3 +436,39 @@ def step(domain: Domain, options: Options, dt_seconds: float, enforce_limits: bo
     """apply_forcing -> advect -> (enforce_limits), time_step.f90:319-389."""
     domain._flush()
     L.check(L.load().icar_adv_step(domain.handle, C.c_double(dt_seconds), int(enforce_limits)), domain.handle)
+
+
+def step_host(domain: Domain, options: Options, dt_seconds: float, q_in: dict, q_out: dict | None = None,
+              enforce_limits: bool = False) -> dict:
+    """One step for species held in host memory (icar_adv_step_host): the
+    arrays of q_in (every advected species, by name) go to the device, the
+    step runs, and the results come back into q_out (new arrays when None;
+    q_out may be q_in).  Uploads, the step and downloads overlap by species
+    group when the arrays are page-locked (e.g. torch pinned tensors'
+    numpy views)."""
+    domain._flush()
+    names = list(domain.adv_vars)
+    missing = [n for n in names if n not in q_in]
+    if missing:
+        raise KeyError(f"q_in lacks {missing}")
+    shape = (domain.ny, domain.nz, domain.nx)
+    ins = []
+    for n in names:
+        a = q_in[n]
+        if a.dtype != np.float32 or not a.flags.c_contiguous or a.shape != shape:
+            raise ValueError(f"{n}: need a C-contiguous float32 array of shape {shape}")
+        ins.append(a)
+    if q_out is None:
+        q_out = {n: np.empty(shape, np.float32) for n in names}
+    outs = []
+    for n in names:
+        a = q_out[n]
+        if a.dtype != np.float32 or not a.flags.c_contiguous or a.shape != shape or not a.flags.writeable:
+            raise ValueError(f"{n}: q_out needs a writeable C-contiguous float32 array of shape {shape}")
+        outs.append(a)
+    k = max(len(names), 1)
+    pin = (C.c_void_p * k)(*[a.ctypes.data for a in ins])
+    pout = (C.c_void_p * k)(*[a.ctypes.data for a in outs])
+    L.check(L.load().icar_adv_step_host(domain.handle, C.c_double(dt_seconds), int(enforce_limits), pin, pout),
+            domain.handle)
+    return q_out

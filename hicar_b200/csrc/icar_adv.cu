@@ -47,6 +47,9 @@ struct icar_adv_domain {
     Geo g{};
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    // icar_adv_step_host: copy streams and per-group events, created on first use
+    cudaStream_t io_in = nullptr, io_out = nullptr;
+    std::vector<cudaEvent_t> io_events;
     size_t n_cell = 0, n_u = 0, n_v = 0, n_zf = 0;
     size_t bytes = 0;
     // resident inputs
@@ -623,10 +626,11 @@ int ensure_fused(icar_adv_t *h)
     return ICAR_ADV_OK;
 }
 
-int mpdata_fused_step(icar_adv_t *h, float dt)
+// Species-independent part of the fused MPDATA step (Courant fluxes, G,
+// DJR, W').
+int mpdata_prep(icar_adv_t *h, float dt)
 {
     const Geo &g = h->g;
-    const int S = h->desc.n_species;
     int e = ensure_fused(h);
     if (e) return e;
     const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
@@ -636,32 +640,46 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
     if (h->opts.debug &&
         icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p, 1))
         return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
+    return check_launch(h, "fused MPDATA prep", 1);
+}
+
+// Donor-cell pass and fused correction for species [s0, s1); results in qn.
+int mpdata_group(icar_adv_t *h, int s0, int s1)
+{
+    const Geo &g = h->g;
+    const int S = s1 - s0;
+    if (S <= 0) return ICAR_ADV_OK;
     icar::SpeciesPtrs sp{};
     for (int s = 0; s < S; s++) {
-        sp.q0[s] = h->q[s].p;
-        sp.q1[s] = h->q1s[s].p;
-        sp.out[s] = h->qn[s].p;
+        sp.q0[s] = h->q[s0 + s].p;
+        sp.q1[s] = h->q1s[s0 + s].p;
+        sp.out[s] = h->qn[s0 + s].p;
     }
     const size_t nc = (size_t)g.nx * g.nz * g.ny;
-    if (S > 0) {
-        const dim3 gu(blocks_for(nc, 256), icar::upwind_ngroups(S, h->sp_group));
-        icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, S, icar::upwind_group(S, h->sp_group), h->Um.p, h->Vm.p,
-                                                     h->Wm.p, h->Gc.p, h->DJR.p);
-        cudaEvent_t c0 = nullptr, c1 = nullptr;
-        if (h->profiling) {
-            cudaEventCreate(&c0);
-            cudaEventCreate(&c1);
-            cudaEventRecord(c0, h->stream);
-        }
-        icar::mp_corr_launch(h->stream, h->mp_shape, g, sp, S, h->opts.mpdata_fct, h->Um.p, h->Vm.p, h->Wp.p,
-                             h->Gc.p, h->DJR.p, h->dz.p);
-        if (h->profiling) {
-            cudaEventRecord(c1, h->stream);
-            h->corr_events.emplace_back(c0, c1);
-        }
+    const dim3 gu(blocks_for(nc, 256), icar::upwind_ngroups(S, h->sp_group));
+    icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, S, icar::upwind_group(S, h->sp_group), h->Um.p, h->Vm.p,
+                                                 h->Wm.p, h->Gc.p, h->DJR.p);
+    cudaEvent_t c0 = nullptr, c1 = nullptr;
+    if (h->profiling) {
+        cudaEventCreate(&c0);
+        cudaEventCreate(&c1);
+        cudaEventRecord(c0, h->stream);
     }
-    e = check_launch(h, "fused MPDATA kernels", S > 0 ? 3 : 1);
+    icar::mp_corr_launch(h->stream, h->mp_shape, g, sp, S, h->opts.mpdata_fct, h->Um.p, h->Vm.p, h->Wp.p, h->Gc.p,
+                         h->DJR.p, h->dz.p);
+    if (h->profiling) {
+        cudaEventRecord(c1, h->stream);
+        h->corr_events.emplace_back(c0, c1);
+    }
+    return check_launch(h, "fused MPDATA kernels", 2);
+}
+
+int mpdata_fused_step(icar_adv_t *h, float dt)
+{
+    const int S = h->desc.n_species;
+    int e = mpdata_prep(h, dt);
     if (e) return e;
+    if ((e = mpdata_group(h, 0, S))) return e;
     for (int s = 0; s < S; s++) std::swap(h->q[s], h->qn[s]);
     return ICAR_ADV_OK;
 }
@@ -686,10 +704,11 @@ int ensure_std_fused(icar_adv_t *h)
     return ICAR_ADV_OK;
 }
 
-int std_fused_step(icar_adv_t *h, float dt)
+// Species-independent part of the fused standard scheme (Courant fluxes,
+// G, DJR).
+int std_prep(icar_adv_t *h, float dt)
 {
     const Geo &g = h->g;
-    const int S = h->desc.n_species;
     int e = ensure_std_fused(h);
     if (e) return e;
     const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
@@ -701,45 +720,60 @@ int std_fused_step(icar_adv_t *h, float dt)
         icar::check_courant(h->stream, h->g, h->Um.p, h->Vm.p, h->Wm.p, h->dz.p, h->jac.p, h->rho.p,
                             h->opts.advect_density))
         return fail(h, ICAR_ADV_CFL_VIOLATION, "a Courant number >= 1 was found (debug check)");
+    return check_launch(h, "fused standard-scheme prep", 1);
+}
+
+// The adv_std_advect3d calls of one step for species [s0, s1); results in
+// q1s with RK3, in qn otherwise.
+int std_group(icar_adv_t *h, int s0, int s1)
+{
+    const Geo &g = h->g;
+    const int S = s1 - s0;
+    if (S <= 0) return ICAR_ADV_OK;
     const int ho = h->opts.h_order, vo = h->opts.v_order, hs = h->hs;
     const bool corr = h->opts.flux_corr == 1;
     auto stage = [&](std::vector<DevBuf> *qf, std::vector<DevBuf> *out, float tf, bool c) {
         icar::SpeciesPtrs sp{};
         for (int s = 0; s < S; s++) {
-            sp.q0[s] = h->q[s].p;
-            sp.q1[s] = (qf ? *qf : h->q)[s].p;
-            sp.out[s] = (*out)[s].p;
+            sp.q0[s] = h->q[s0 + s].p;
+            sp.q1[s] = (qf ? *qf : h->q)[s0 + s].p;
+            sp.out[s] = (*out)[s0 + s].p;
         }
         return icar::std_fused_launch(h->stream, c, ho, vo, g, hs, tf, sp, S, h->Um.p, h->Vm.p, h->Wm.p, h->Gc.p,
                                       h->DJR.p);
     };
     cudaEvent_t c0 = nullptr, c1 = nullptr;
-    if (h->profiling && S > 0) {
+    if (h->profiling) {
         cudaEventCreate(&c0);
         cudaEventCreate(&c1);
         cudaEventRecord(c0, h->stream);
     }
-    int bad = 0, nl = 1;
-    if (S > 0) {
-        if (h->opts.rk3) {
-            // advection_driver.f90:100-110: q + 1/3, q + 1/2 from the first
-            // result, then the full step (with the flux correction) from the second
-            bad |= stage(nullptr, &h->q1s, 0.333f, false);
-            bad |= stage(&h->q1s, &h->qn, 0.5f, false);
-            bad |= stage(&h->qn, &h->q1s, 1.0f, corr);
-            nl += 6;
-        } else {
-            bad |= stage(nullptr, &h->qn, 1.0f, corr);
-            nl += 2;
-        }
+    int bad = 0, nl = 0;
+    if (h->opts.rk3) {
+        // advection_driver.f90:100-110: q + 1/3, q + 1/2 from the first
+        // result, then the full step (with the flux correction) from the second
+        bad |= stage(nullptr, &h->q1s, 0.333f, false);
+        bad |= stage(&h->q1s, &h->qn, 0.5f, false);
+        bad |= stage(&h->qn, &h->q1s, 1.0f, corr);
+        nl = 6;
+    } else {
+        bad |= stage(nullptr, &h->qn, 1.0f, corr);
+        nl = 2;
     }
-    if (h->profiling && S > 0) {
+    if (h->profiling) {
         cudaEventRecord(c1, h->stream);
         h->corr_events.emplace_back(c0, c1);
     }
     if (bad) return fail(h, ICAR_ADV_BAD_ARG, "h_order and v_order must be 1, 3 or 5");
-    e = check_launch(h, "fused standard-scheme kernels", nl);
+    return check_launch(h, "fused standard-scheme kernels", nl);
+}
+
+int std_fused_step(icar_adv_t *h, float dt)
+{
+    const int S = h->desc.n_species;
+    int e = std_prep(h, dt);
     if (e) return e;
+    if ((e = std_group(h, 0, S))) return e;
     for (int s = 0; s < S; s++) std::swap(h->q[s], h->opts.rk3 ? h->q1s[s] : h->qn[s]);
     return ICAR_ADV_OK;
 }
@@ -947,6 +981,11 @@ int icar_adv_destroy(icar_adv_t *h)
     for (auto &b : h->dqdt) release(b);
     if (h->filter_dev) cudaFree(h->filter_dev);
     if (h->zone_dev) cudaFree(h->zone_dev);
+    if (h->io_in) cudaStreamSynchronize(h->io_in);
+    if (h->io_out) cudaStreamSynchronize(h->io_out);
+    for (cudaEvent_t ev : h->io_events) cudaEventDestroy(ev);
+    if (h->io_in) cudaStreamDestroy(h->io_in);
+    if (h->io_out) cudaStreamDestroy(h->io_out);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
     return ICAR_ADV_OK;
@@ -1204,6 +1243,120 @@ int icar_adv_set_precipitation(icar_adv_t *h, const double *rain, const double *
         else
             CUDA_TRY(h, cudaMemsetAsync(dst, 0, n2 * sizeof(double), h->stream));
     }
+    return icar_adv_sync(h);
+}
+
+namespace {
+
+// apply_forcing for species [s0, s1) (icar_adv_apply_forcing over a range).
+int forcing_range(icar_adv_t *h, double dt_seconds, int s0, int s1)
+{
+    if (h->nzone == 0) return ICAR_ADV_OK;
+    const size_t n = (size_t)h->nzone * h->g.nz;
+    int launched = 0;
+    for (int s = s0; s < s1; s++) {
+        if (!h->forcing[s].p) continue;
+        launched++;
+        if (!h->dqdt[s].p) {
+            int e = alloc(h, h->dqdt[s], h->n_cell);  // zero tendency: fixed inflow
+            if (e) return e;
+        }
+        icar::k_apply_forcing<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->g, h->nzone, h->zone_dev, h->filter_dev,
+                                                                          dt_seconds, h->q[s].p, h->forcing[s].p,
+                                                                          h->dqdt[s].p);
+    }
+    return check_launch(h, "apply_forcing", launched);
+}
+
+// Species groups of icar_adv_step_host: one species per group up to 12 (on
+// config 2 the step then runs within about 10 % of the page-locked copy
+// time; 4 groups left 20 % more exposed).
+constexpr int IO_GROUPS = 12;
+
+int copy_species_async(icar_adv_t *h, float *dev, float *host, bool to_device, cudaStream_t st)
+{
+    const size_t P = (size_t)h->g.P, ex = (size_t)h->g.nx, rows = (size_t)h->g.nz * h->g.ny;
+    cudaError_t ce = to_device ? cudaMemcpy2DAsync(dev, P * 4, host, ex * 4, ex * 4, rows, cudaMemcpyHostToDevice, st)
+                               : cudaMemcpy2DAsync(host, ex * 4, dev, P * 4, ex * 4, rows, cudaMemcpyDeviceToHost, st);
+    if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaMemcpy2DAsync: %s", cudaGetErrorString(ce));
+    return ICAR_ADV_OK;
+}
+
+}  // namespace
+
+int icar_adv_step_host(icar_adv_t *h, double dt_seconds, int32_t enforce_limits, const float *const *q_in,
+                       float *const *q_out)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (h->batch) return fail(h, ICAR_ADV_BAD_ARG, "domain is a batch member: step it with icar_adv_batch_step");
+    const int S = h->desc.n_species;
+    if (S > 0 && (!q_in || !q_out)) return fail(h, ICAR_ADV_BAD_ARG, "species pointer list is NULL");
+    for (int s = 0; s < S; s++)
+        if (!q_in[s] || !q_out[s]) return fail(h, ICAR_ADV_BAD_ARG, "species %d host pointer is NULL", s);
+    if (!std::isfinite(dt_seconds)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite");
+    cudaSetDevice(h->desc.device);
+    const bool mp = h->opts.advection == ICAR_ADV_MPDATA;
+    const bool fused_mp = mp && !h->opts.rk3 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct);
+    int e;
+    if (h->path != 0 || !(fused_mp || !mp) || h->opts.debug || S == 0) {
+        // the unpipelined sequence (staged kernels, debug checks, RK3 MPDATA)
+        for (int s = 0; s < S; s++)
+            if ((e = copy_field(h, h->desc.species[s], const_cast<float *>(q_in[s]), nullptr, true))) return e;
+        if ((e = icar_adv_step(h, dt_seconds, enforce_limits))) return e;
+        for (int s = 0; s < S; s++)
+            if ((e = copy_field(h, h->desc.species[s], q_out[s], nullptr, false, false))) return e;
+        return icar_adv_sync(h);
+    }
+    const int ngroups = std::min(S, IO_GROUPS);
+    if (!h->io_in) {
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&h->io_in, cudaStreamNonBlocking));
+        CUDA_TRY(h, cudaStreamCreateWithFlags(&h->io_out, cudaStreamNonBlocking));
+        h->io_events.assign(2 * IO_GROUPS + 1, nullptr);
+        for (auto &ev : h->io_events) CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    cudaEvent_t ev_start = h->io_events[2 * IO_GROUPS];
+    // uploads start once the work already queued on the handle's stream is done
+    CUDA_TRY(h, cudaEventRecord(ev_start, h->stream));
+    CUDA_TRY(h, cudaStreamWaitEvent(h->io_in, ev_start, 0));
+    for (int s = 0; s < S; s++) h->have_q[s] = true;
+    if ((e = ensure_ready(h))) return e;
+    const float dt = (float)dt_seconds;
+    if ((e = mp ? mpdata_prep(h, dt) : std_prep(h, dt))) return e;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t before = h->launches;
+    if (h->profiling) {
+        cudaEventCreate(&ev0);
+        cudaEventCreate(&ev1);
+        cudaEventRecord(ev0, h->stream);
+    }
+    auto result = [&](int s) -> DevBuf & { return mp ? h->qn[s] : (h->opts.rk3 ? h->q1s[s] : h->qn[s]); };
+    for (int gi = 0; gi < ngroups; gi++) {
+        const int s0 = S * gi / ngroups, s1 = S * (gi + 1) / ngroups;
+        cudaEvent_t ev_in = h->io_events[gi], ev_done = h->io_events[IO_GROUPS + gi];
+        for (int s = s0; s < s1; s++)
+            if ((e = copy_species_async(h, h->q[s].p, const_cast<float *>(q_in[s]), true, h->io_in))) return e;
+        CUDA_TRY(h, cudaEventRecord(ev_in, h->io_in));
+        CUDA_TRY(h, cudaStreamWaitEvent(h->stream, ev_in, 0));
+        if ((e = forcing_range(h, dt_seconds, s0, s1))) return e;
+        if ((e = mp ? mpdata_group(h, s0, s1) : std_group(h, s0, s1))) return e;
+        if (enforce_limits) {
+            for (int s = s0; s < s1; s++)
+                icar::k_enforce_limits<<<blocks_for(h->n_cell, 256), 256, 0, h->stream>>>(h->g, result(s).p);
+            if ((e = check_launch(h, "enforce_limits", s1 - s0))) return e;
+        }
+        CUDA_TRY(h, cudaEventRecord(ev_done, h->stream));
+        CUDA_TRY(h, cudaStreamWaitEvent(h->io_out, ev_done, 0));
+        for (int s = s0; s < s1; s++)
+            if ((e = copy_species_async(h, result(s).p, q_out[s], false, h->io_out))) return e;
+    }
+    if (h->profiling) {
+        cudaEventRecord(ev1, h->stream);
+        h->events.emplace_back(ev0, ev1);
+        h->timed_launches += h->launches - before;
+    }
+    CUDA_TRY(h, cudaStreamSynchronize(h->io_out));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (int s = 0; s < S; s++) std::swap(h->q[s], result(s));
     return icar_adv_sync(h);
 }
 

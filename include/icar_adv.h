@@ -191,6 +191,21 @@ int icar_adv_enforce_limits(icar_adv_t *h);
  * enforce_limits != 0.  Asynchronous on the handle's stream. */
 int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits);
 
+/* The same step for a caller whose species live in host memory, as the
+ * reference's advect(domain, options, dt) sees them when CPU physics runs
+ * between calls: q_in[s] holds species s (adv_vars order, contiguous
+ * Fortran order) before the step, q_out[s] receives it after (q_out[s] may
+ * equal q_in[s]).  Equivalent to icar_adv_set_field of every species,
+ * icar_adv_step, then icar_adv_get_field of every species, with the same
+ * results bit for bit; on the fused kernels the species go in groups (one
+ * species each, up to 12 groups) so that the uploads of one group, the
+ * step of the previous one and the downloads of the one before overlap
+ * (copy streams of their own, which needs page-locked host arrays;
+ * pageable ones are copied without overlap).  Returns when q_out is
+ * complete. */
+int icar_adv_step_host(icar_adv_t *h, double dt_seconds, int32_t enforce_limits, const float *const *q_in,
+                       float *const *q_out);
+
 /* balance_uvw(domain, options), src/physics/wind.f90:88-164, called every
  * step before advection when advect_density is set (time_step.f90:324):
  * rebuilds the resident w from the horizontal divergence of the resident u
