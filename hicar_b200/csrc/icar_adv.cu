@@ -1133,7 +1133,9 @@ int icar_adv_balance_uvw(icar_adv_t *h)
     if (missing) return fail(h, ICAR_ADV_NOT_READY, "field %s was never set", missing);
     const Geo &g = h->g;
     const float *rho = adv_den ? h->rho.p : h->jac.p;  // only read when advect_density
-    icar::k_balance_uvw<<<blocks_for((size_t)g.nx * g.ny, 128), 128, 0, h->stream>>>(
+    const dim3 grid((unsigned)((g.nx + icar::balf::BX - 1) / icar::balf::BX),
+                    (unsigned)((g.ny + icar::balf::BY - 1) / icar::balf::BY));
+    icar::k_balance_uvw<<<grid, icar::balf::NT, icar::balf::SMEM, h->stream>>>(
         g, h->hs, h->desc.dx, adv_den, h->u.p, h->v.p, rho, h->dz.p, h->jac_u.p, h->jac_v.p, h->jac_w.p, h->w.p);
     h->have_w = true;
     return check_launch(h, "balance_uvw");

@@ -5,7 +5,8 @@
 //                   calc_divergence(horz_only) and calc_w (:166-271): one
 //                   thread per (i, j) column marches up the column, forming
 //                   the horizontal divergence of the metric-weighted u, v at
-//                   each level and integrating w from w = 0 below the ground.
+//                   each level and integrating w from w = 0 below the ground;
+//                   the levels arrive in shared-memory planes ahead of use.
 //   k_dt_maxima     the maxima compute_dt (src/main/time_step.f90:51-168)
 //                   needs: max |u|, |v|, |w| over the whole arrays and the
 //                   per-cell CFL rate max(|u|/dx, |v|/dx, |w|/dz) over the
@@ -18,84 +19,155 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "mpdata_fused.cuh"
 
 namespace icar {
 
+namespace balf {
+// CTA tile: 32 x 8 columns, one thread per column marching up k.  The
+// seven fields a level needs (u, J_u, v, J_v, rho, dz, J_w) arrive in
+// shared-memory planes by 16-byte cp.async, DEPTH levels ahead of use:
+// each plane spans x from i0-4 (a multiple of 4) to i0+35 and y from j0-1
+// to j0+8, covering the faces i0..i0+32 / j0..j0+8 and the density
+// neighbours the face weights read.
+constexpr int BX = 32, BY = 8, NT = BX * BY;
+constexpr int PW = 40, PH = BY + 2, PLANE = PW * PH;
+constexpr int NF = 7;                      // u, ju, v, jv, rho, dz, jw
+constexpr int DEPTH = 3, NSLOT = DEPTH + 1;
+constexpr int CPR = PW / 4, NCH = (NF * CPR * PH + NT - 1) / NT;
+constexpr size_t SMEM = (size_t)NSLOT * NF * PLANE * sizeof(float);
+}  // namespace balf
+
 // u*J_u on x face f, times the face density when advect_density (the
-// outermost faces extrapolate it), wind.f90:237-239.
-__device__ __forceinline__ float umet(const Geo &g, int adv_den, const float *__restrict__ u,
-                                      const float *__restrict__ ju, const float *__restrict__ rho, int f, int k, int j)
+// outermost faces extrapolate it), wind.f90:237-239.  U, JU, R point at
+// the cell's row of the u, J_u and density planes; plane column = index -
+// ox.
+__device__ __forceinline__ float umet_p(int nx, int adv_den, const float *U, const float *JU, const float *R, int f,
+                                        int ox)
 {
-    const size_t c = ix(g, f, k, j);
-    const float uj = u[c] * ju[c];
+    const int p = f - ox;
+    const float uj = U[p] * JU[p];
     if (!adv_den) return uj;
-    if (f == 0) return uj * (1.5f * rho[ix(g, 0, k, j)] - 0.5f * rho[ix(g, 1, k, j)]);
-    if (f == g.nx) return uj * (1.5f * rho[ix(g, g.nx - 1, k, j)] - 0.5f * rho[ix(g, g.nx - 2, k, j)]);
-    return uj * (rho[c - 1] + rho[c]) / 2.0f;
+    if (f == 0) return uj * (1.5f * R[0 - ox] - 0.5f * R[1 - ox]);
+    if (f == nx) return uj * (1.5f * R[nx - 1 - ox] - 0.5f * R[nx - 2 - ox]);
+    return uj * (R[p - 1] + R[p]) / 2.0f;
 }
 
-// v*J_v on y face gy, wind.f90:241-243.
-__device__ __forceinline__ float vmet(const Geo &g, int adv_den, const float *__restrict__ v,
-                                      const float *__restrict__ jv, const float *__restrict__ rho, int i, int k, int gy)
+// v*J_v on y face gy, wind.f90:241-243; V, JV, R point at row gy of the v,
+// J_v and density planes in the cell's column (rows of stride balf::PW).
+__device__ __forceinline__ float vmet_p(int ny, int adv_den, const float *V, const float *JV, const float *R, int gy)
 {
-    const size_t c = ix(g, i, k, gy);
-    const float vj = v[c] * jv[c];
+    constexpr int W = balf::PW;
+    const float vj = V[0] * JV[0];
     if (!adv_den) return vj;
-    if (gy == 0) return vj * (1.5f * rho[ix(g, i, k, 0)] - 0.5f * rho[ix(g, i, k, 1)]);
-    if (gy == g.ny) return vj * (1.5f * rho[ix(g, i, k, g.ny - 1)] - 0.5f * rho[ix(g, i, k, g.ny - 2)]);
-    return vj * (rho[ix(g, i, k, gy - 1)] + rho[c]) / 2.0f;
+    if (gy == 0) return vj * (1.5f * R[0] - 0.5f * R[W]);
+    if (gy == ny) return vj * (1.5f * R[-W] - 0.5f * R[-2 * W]);
+    return vj * (R[-W] + R[0]) / 2.0f;
 }
 
 // Columns i_s..i_e x j_s..j_e (its-1..ite+1 clipped to the domain, i.e.
 // [max(hs-1,0), min(n-hs,n-1)] for one image with halo hs) get the balanced
 // w; every other column gets w = 0 (calc_w sets the whole array first).
-__global__ void k_balance_uvw(Geo g, int hs, float dx, int adv_den, const float *__restrict__ u,
-                              const float *__restrict__ v, const float *__restrict__ rho,
-                              const float *__restrict__ dz, const float *__restrict__ ju,
-                              const float *__restrict__ jv, const float *__restrict__ jw, float *__restrict__ w)
+__global__ void __launch_bounds__(balf::NT)
+    k_balance_uvw(Geo g, int hs, float dx, int adv_den, const float *__restrict__ u, const float *__restrict__ v,
+                  const float *__restrict__ rho, const float *__restrict__ dz, const float *__restrict__ ju,
+                  const float *__restrict__ jv, const float *__restrict__ jw, float *__restrict__ w)
 {
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (int)(t % (size_t)g.nx);
-    const int j = (int)(t / (size_t)g.nx);
-    if (j >= g.ny) return;
-    const int i_s = max(hs - 1, 0), i_e = min(g.nx - hs, g.nx - 1);
-    const int j_s = max(hs - 1, 0), j_e = min(g.ny - hs, g.ny - 1);
-    const int nz = g.nz;
-    if (i < i_s || i > i_e || j < j_s || j > j_e) {
-        for (int k = 0; k < nz; k++) w[ix(g, i, k, j)] = 0.0f;
-        return;
+    using namespace balf;
+    extern __shared__ float4 sm4[];
+    float *sm = reinterpret_cast<float *>(sm4);
+    const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int ox = i0 - 4, oy = j0 - 1;
+    const int i_s = max(hs - 1, 0), i_e = min(nx - hs, nx - 1);
+    const int j_s = max(hs - 1, 0), j_e = min(ny - hs, ny - 1);
+    const bool in = i < nx && j < ny;
+    const bool bal = in && i >= i_s && i <= i_e && j >= j_s && j <= j_e;
+    // every thread's chunks of one level: field f, row ly, chunk cx
+    const float *src[NCH];
+    size_t off[NCH];
+    int dst[NCH];
+    bool ok[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        const int e = threadIdx.x + c * NT;
+        dst[c] = -1;
+        ok[c] = false;
+        off[c] = 0;
+        src[c] = u;
+        if (e < NF * CPR * PH) {
+            const int f = e / (CPR * PH), r = e % (CPR * PH);
+            const int ly = r / CPR, cx = r % CPR;
+            const int gi = ox + 4 * cx, gj = oy + ly;
+            const bool yface = f == 2 || f == 3;
+            dst[c] = f * PLANE + ly * PW + 4 * cx;
+            src[c] = f == 0 ? u : f == 1 ? ju : f == 2 ? v : f == 3 ? jv : f == 4 ? rho : f == 5 ? dz : jw;
+            ok[c] = gi >= 0 && gi < g.P && gj >= 0 && gj < (yface ? ny + 1 : ny);
+            if (ok[c]) off[c] = (size_t)gi + (size_t)g.P * nz * gj;
+        }
     }
-    float wb = 0.0f, rib = 0.0f;  // w and the interface density one level down
+    auto issue = [&](int k) {
+        if (k < nz) {
+            float *slot = sm + (size_t)(k % NSLOT) * NF * PLANE;
+            const size_t lo = (size_t)k * g.P;
+#pragma unroll
+            for (int c = 0; c < NCH; c++)
+                if (dst[c] >= 0) cp_async16(slot + dst[c], ok[c] ? src[c] + off[c] + lo : src[c], ok[c]);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) issue(k);
+    float wb = 0.0f, rib = 0.0f, jwb = 0.0f;  // w, interface density and J_w one level down
+    const int px = i - ox, py = j - oy;
     for (int k = 0; k < nz; k++) {
+        cp_async_wait<DEPTH - 2>();  // levels k and k+1 have landed
+        __syncthreads();
+        issue(k + DEPTH);            // into the slot of level k-1, read by nobody any more
+        const float *L = sm + (size_t)(k % NSLOT) * NF * PLANE;
+        const float *Lu = sm + (size_t)((k + 1) % NSLOT) * NF * PLANE;
         const size_t c = ix(g, i, k, j);
-        const float ue = umet(g, adv_den, u, ju, rho, i + 1, k, j), uw = umet(g, adv_den, u, ju, rho, i, k, j);
-        const float vn = vmet(g, adv_den, v, jv, rho, i, k, j + 1), vs = vmet(g, adv_den, v, jv, rho, i, k, j);
+        if (!bal) {
+            if (in) w[c] = 0.0f;
+            continue;
+        }
+        const float *U = L, *JU = L + PLANE, *V = L + 2 * PLANE, *JV = L + 3 * PLANE, *R = L + 4 * PLANE;
+        const float *DZ = L + 5 * PLANE, *JW = L + 6 * PLANE;
+        const float *Ur = U + py * PW, *JUr = JU + py * PW, *Rr = R + py * PW;
+        const float ue = umet_p(nx, adv_den, Ur, JUr, Rr, i + 1, ox), uw = umet_p(nx, adv_den, Ur, JUr, Rr, i, ox);
+        const int pc = py * PW + px;
+        const float vn = vmet_p(ny, adv_den, V + pc + PW, JV + pc + PW, R + pc + PW, j + 1);
+        const float vs = vmet_p(ny, adv_den, V + pc, JV + pc, R + pc, j);
         const float div = ((ue - uw) + (vn - vs)) / dx;
-        const float d = dz[c], jwc = jw[c];
+        const float d = DZ[pc], jwc = JW[pc];
         float wk;
         if (adv_den) {
             // rho_i(k) = (rho_k*dz_k + rho_k+1*dz_k+1) / (dz_k + dz_k+1), wind.f90:175-176
             float ri = 0.0f;
             if (k < nz - 1) {
-                const size_t cu = c + (size_t)g.P;
-                ri = (rho[c] * d + rho[cu] * dz[cu]) / (d + dz[cu]);
+                const float dzu = Lu[5 * PLANE + pc];
+                ri = (R[pc] * d + Lu[4 * PLANE + pc] * dzu) / (d + dzu);
             }
             if (k == 0)
                 wk = 0.0f - div * d / (jwc * ri);
             else if (k == nz - 1)
-                wk = ((wb * rib * jw[c - (size_t)g.P]) - div * d) / (jwc * rho[c]);
+                wk = ((wb * rib * jwb) - div * d) / (jwc * R[pc]);
             else
-                wk = ((wb * rib * jw[c - (size_t)g.P]) - div * d) / (jwc * ri);
+                wk = ((wb * rib * jwb) - div * d) / (jwc * ri);
             rib = ri;
         } else {
             if (k == 0)
                 wk = (0.0f - div * d) / jwc;
             else
-                wk = (wb * jw[c - (size_t)g.P] - div * d) / jwc;
+                wk = (wb * jwb - div * d) / jwc;
         }
         w[c] = wk;
         wb = wk;
+        jwb = jwc;
     }
+    cp_async_wait<0>();
 }
 
 // out[0..2] = bits of max |u|, |v|, |w| over the arrays; out[3] = bits of
