@@ -1206,9 +1206,11 @@ int icar_adv_mp_simple(icar_adv_t *h, float dt)
     const float cloud2snow = std::exp(-1.0f * (1.0f / 2000.0f) * dt);
     const float cloud2rain = std::exp(-1.0f * (1.0f / 500.0f) * dt);
     const int hs = h->hs;
-    const size_t ncol = (size_t)std::max(g.nx - 2 * hs, 0) * (size_t)std::max(g.ny - 2 * hs, 0);
-    if (ncol > 0)
-        icar::k_mp_simple<<<blocks_for(ncol, 128), 128, 0, h->stream>>>(
+    const int ti = std::max(g.nx - 2 * hs, 0), tj = std::max(g.ny - 2 * hs, 0);
+    if (ti > 0 && tj > 0)
+        icar::k_mp_simple<<<dim3((unsigned)((ti + icar::mpsf::BX - 1) / icar::mpsf::BX),
+                                 (unsigned)((tj + icar::mpsf::BY - 1) / icar::mpsf::BY)),
+                            icar::mpsf::NT, icar::mpsf::SMEM, h->stream>>>(
             g, hs, dt, cloud2rain, cloud2snow, h->pressure.p, h->q[s_th].p, h->exner.p, h->rho.p, h->q[s_qv].p,
             h->q[s_qc].p, h->q[s_qr].p, h->q[s_qs].p, h->dz_mass.p, h->acc_precip, h->acc_precip + n2, h->mp_stop);
     h->mp_ran = true;

@@ -6,7 +6,10 @@
 // Phase 1 walks up the column doing the per-level conversions
 // (mp_conversions: saturation adjustment by the reference's iteration,
 // autoconversion, melting, evaporation and sublimation with latent-heat
-// feedback) and leaves the air temperature T = th*pii in the th array.
+// feedback), its inputs arriving in shared-memory planes by cp.async three
+// levels ahead; it leaves the air temperature T = th*pii in the th array
+// and forms on the way the column maxima the sedimentation passes start
+// from (in the reference's order, level 0 first).
 // Phases 2 and 3 sediment rain and then snow in CFL substeps (sediment, as a
 // single upward sweep: each level's downward flux is formed from the level
 // above before that level is touched, exactly the reference's values and
@@ -24,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "mpdata_fused.cuh"
 
 namespace icar {
 namespace mps {
@@ -146,43 +150,113 @@ __device__ __forceinline__ void mp_conversions(float pressure, float &temperatur
     }
 }
 
-// One column.  T lives in th between the phases.
-__global__ void k_mp_simple(Geo g, int hs, float dt, float cloud2rain, float cloud2snow,
-                            const float *__restrict__ pressure, float *__restrict__ th,
-                            const float *__restrict__ pii, const float *__restrict__ rho, float *__restrict__ qv,
-                            float *__restrict__ qc, float *__restrict__ qr, float *__restrict__ qs,
-                            const float *__restrict__ dz, double *__restrict__ acc_rain,
-                            double *__restrict__ acc_snow, int *__restrict__ stop_flag)
+namespace mpsf {
+// CTA tile of 32 x 4 columns; the planes of one level span x from
+// floor4(i0) to +35 (a multiple of 4, so 16-byte chunks).
+constexpr int BX = 32, BY = 4, NT = BX * BY;
+constexpr int PW = 36, PH = BY, PLANE = PW * PH;   // x from floor4(i0) to +35
+constexpr int NF = 8;                               // pressure, th, pii, qv, qc, qr, qs, dz
+constexpr int DEPTH = 3, NSLOT = DEPTH + 1;
+constexpr int CPR = PW / 4, NCH = (NF * CPR * PH + NT - 1) / NT;
+constexpr size_t SMEM = (size_t)NSLOT * NF * PLANE * sizeof(float);
+}  // namespace mpsf
+
+// One column per thread; phase 1 reads its levels from shared-memory planes
+// filled by cp.async ahead of use.  T lives in th between the phases.
+__global__ void __launch_bounds__(mpsf::NT)
+    k_mp_simple(Geo g, int hs, float dt, float cloud2rain, float cloud2snow,
+                const float *__restrict__ pressure, float *__restrict__ th, const float *__restrict__ pii,
+                const float *__restrict__ rho, float *__restrict__ qv, float *__restrict__ qc,
+                float *__restrict__ qr, float *__restrict__ qs, const float *__restrict__ dz,
+                double *__restrict__ acc_rain, double *__restrict__ acc_snow, int *__restrict__ stop_flag)
 {
-    const int ti = g.nx - 2 * hs;
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ti <= 0 || t >= (size_t)ti * (size_t)(g.ny - 2 * hs)) return;
-    const int i = hs + (int)(t % (size_t)ti), j = hs + (int)(t / (size_t)ti);
+    using namespace mpsf;
+    extern __shared__ float4 sm4[];
+    float *sm = reinterpret_cast<float *>(sm4);
+    const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
+    const int i0 = hs + blockIdx.x * BX, j0 = hs + blockIdx.y * BY;
+    const int i = i0 + tx, j = j0 + ty;
+    const int ox = i0 - (i0 & 3), oy = j0;
+    const bool col = i < g.nx - hs && j < g.ny - hs;
     const int nz = g.nz;
-    const size_t st = (size_t)g.P, c0 = ix(g, i, 0, j);
+    const size_t st = (size_t)g.P, c0 = col ? ix(g, i, 0, j) : 0;
     int stop = 0;
+    const float *src[NCH];
+    size_t off[NCH];
+    int dst[NCH];
+    bool ok[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        const int e = threadIdx.x + c * NT;
+        dst[c] = -1;
+        ok[c] = false;
+        off[c] = 0;
+        src[c] = pressure;
+        if (e < NF * CPR * PH) {
+            const int f = e / (CPR * PH), r = e % (CPR * PH);
+            const int ly = r / CPR, cx = r % CPR;
+            const int gi = ox + 4 * cx, gj = oy + ly;
+            dst[c] = f * PLANE + ly * PW + 4 * cx;
+            src[c] = f == 0 ? pressure : f == 1 ? th : f == 2 ? pii : f == 3 ? qv : f == 4 ? qc : f == 5 ? qr : f == 6 ? qs : dz;
+            ok[c] = gi < g.P && gj < g.ny;
+            if (ok[c]) off[c] = (size_t)gi + (size_t)g.P * nz * gj;
+        }
+    }
+    auto issue = [&](int k) {
+        if (k < nz) {
+            float *slot = sm + (size_t)(k % NSLOT) * NF * PLANE;
+            const size_t lo = (size_t)k * g.P;
+#pragma unroll
+            for (int c = 0; c < NCH; c++)
+                if (dst[c] >= 0) cp_async16(slot + dst[c], ok[c] ? src[c] + off[c] + lo : src[c], ok[c]);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) issue(k);
+    const int pc = ty * PW + (i - ox);
+    // column maxima the sedimentation passes start from, formed in the
+    // reference's order (level 0 first) while the levels go by
+    float mx_r = 0.0f, mx_s = 0.0f, m_r = 0.0f, m_s = 0.0f;
     // phase 1: conversions level by level
     for (int k = 0; k < nz; k++) {
+        cp_async_wait<DEPTH - 1>();
+        __syncthreads();
+        issue(k + DEPTH);
+        if (!col) continue;
+        const float *L = sm + (size_t)(k % NSLOT) * NF * PLANE + pc;
         const size_t c = c0 + k * st;
-        float T = th[c] * pii[c];
-        float v = qv[c], cw = qc[c], r = qr[c], s = qs[c];
-        mp_conversions(pressure[c], T, v, cw, r, s, cloud2rain, cloud2snow, stop);
+        float T = L[PLANE] * L[2 * PLANE];
+        float v = L[3 * PLANE], cw = L[4 * PLANE], r = L[5 * PLANE], s = L[6 * PLANE];
+        mp_conversions(L[0], T, v, cw, r, s, cloud2rain, cloud2snow, stop);
+        const float dzk = dt / L[7 * PLANE];
+        if (k == 0) {
+            mx_r = r;
+            mx_s = s;
+            m_r = dzk * mps::RAIN_FALL;
+            m_s = dzk * mps::SNOW_FALL;
+        } else {
+            mx_r = fmax_(mx_r, r);
+            mx_s = fmax_(mx_s, s);
+            m_r = fmax_(m_r, dzk * mps::RAIN_FALL);
+            m_s = fmax_(m_s, dzk * mps::SNOW_FALL);
+        }
         th[c] = T;
         qv[c] = v;
         qc[c] = cw;
         qr[c] = r;
         qs[c] = s;
     }
+    cp_async_wait<0>();
+    if (!col) return;
     float rain = 0.0f, snow = 0.0f;
     // phases 2 and 3: sedimentation of rain, then of snow
     for (int pass = 0; pass < 2; pass++) {
         float *__restrict__ q = pass == 0 ? qr : qs;
         const float fall = pass == 0 ? mps::RAIN_FALL : mps::SNOW_FALL;
-        float mx = q[c0];
-        for (int k = 1; k < nz; k++) mx = fmax_(mx, q[c0 + k * st]);
+        const float mx = pass == 0 ? mx_r : mx_s;
         if (!(mx > mps::SMALL)) continue;
-        float m = dt / dz[c0] * fall;
-        for (int k = 1; k < nz; k++) m = fmax_(m, dt / dz[c0 + k * st] * fall);
+        const float m = pass == 0 ? m_r : m_s;
         const float cfl = ceilf(m);
         const float fall_rate = dt * fall / cfl;
         const int nsub = (int)lrintf(cfl);
@@ -210,14 +284,18 @@ __global__ void k_mp_simple(Geo g, int hs, float dt, float cloud2rain, float clo
                 snow = snow + sed;
                 rain = rain + sed;
             }
-            // evaporate / sublimate what reached unsaturated levels
+            // evaporate / sublimate what reached unsaturated levels; the
+            // saturation mixing ratio is only formed where there is
+            // something to evaporate (it has no other effect)
             for (int k = 0; k < nz; k++) {
                 const size_t c = c0 + k * st;
+                float h = q[c];
+                if (!(h > mps::SMALL)) continue;
                 float T = th[c];
                 const float L_evap = -1.0f * (mps::LH_VAPOR + (373.15f - T) * mps::DLHVDT);
                 const float qvsat = mp_sat_mr(T, pressure[c]);
-                float v = qv[c], h = q[c];
-                if (v < qvsat && h > mps::SMALL) {
+                float v = qv[c];
+                if (v < qvsat) {
                     mp_phase_change(T, h, qvsat, v, pass == 0 ? L_evap : -1.0f * mps::LH_LIQUID + L_evap, rate,
                                     stop);
                     th[c] = T;
