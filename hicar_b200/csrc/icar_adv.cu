@@ -655,10 +655,11 @@ int mpdata_group(icar_adv_t *h, int s0, int s1)
         sp.q1[s] = h->q1s[s0 + s].p;
         sp.out[s] = h->qn[s0 + s].p;
     }
-    const size_t nc = (size_t)g.nx * g.nz * g.ny;
-    const dim3 gu(blocks_for(nc, 256), icar::upwind_ngroups(S, h->sp_group));
-    icar::k_mp_upwind<<<gu, 256, 0, h->stream>>>(g, sp, S, icar::upwind_group(S, h->sp_group), h->Um.p, h->Vm.p,
-                                                 h->Wm.p, h->Gc.p, h->DJR.p);
+    const int sg = std::min(icar::upwind_group(S, h->sp_group), icar::upf::SGMAX);
+    const dim3 gu((unsigned)((g.nx + icar::upf::BX - 1) / icar::upf::BX),
+                  (unsigned)((g.ny + icar::upf::BY - 1) / icar::upf::BY), (unsigned)((S + sg - 1) / sg));
+    icar::k_mp_upwind_cols<<<gu, icar::upf::NT, icar::upf::SMEM, h->stream>>>(g, sp, S, sg, h->Um.p, h->Vm.p, h->Wm.p,
+                                                                            h->Gc.p, h->DJR.p);
     cudaEvent_t c0 = nullptr, c1 = nullptr;
     if (h->profiling) {
         cudaEventCreate(&c0);

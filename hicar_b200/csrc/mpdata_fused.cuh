@@ -198,6 +198,137 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// Donor-cell pass 1 for every species of a species group, one thread per
+// column marching up the column (the same arithmetic as mp_upwind_at, cell
+// for cell).  CTA tile 32 x 8 columns; blockIdx.z selects the species
+// group.  Each level of every species of the group, and of U_m and V_m,
+// arrives in shared-memory planes by 16-byte cp.async three levels ahead
+// (planes span x from i0-4 to i0+35 and y from j0-1 to j0+8, covering the
+// stencil's x/y neighbours); the vertical neighbours come from the planes
+// of the levels above and below, W_m, G and DJR from the column itself.
+// Boundary-ring columns copy q0 to the pass-1 and output buffers.
+namespace upf {
+constexpr int BX = 32, BY = 8, NT = BX * BY;
+constexpr int PW = 40, PH = BY + 2, PLANE = PW * PH, CPR = PW / 4;
+constexpr int SGMAX = 6;                 // species per CTA
+constexpr int NSL = 5;                   // level slots: k-1 .. k+3
+constexpr int NPL = SGMAX + 2;           // species planes, then U_m, V_m
+constexpr int NCH = (NPL * CPR * PH + NT - 1) / NT;
+constexpr size_t SMEM = (size_t)NSL * NPL * PLANE * sizeof(float);
+}  // namespace upf
+
+__global__ void __launch_bounds__(upf::NT)
+    k_mp_upwind_cols(Geo g, const __grid_constant__ SpeciesPtrs sp, int S, int sg, const float *__restrict__ U,
+                     const float *__restrict__ V, const float *__restrict__ W, const float *__restrict__ Gc,
+                     const float *__restrict__ DJR)
+{
+    using namespace upf;
+    extern __shared__ float4 sm4[];
+    float *sm = reinterpret_cast<float *>(sm4);
+    const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const int s0 = blockIdx.z * sg, n = min(sg, S - s0);
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int ox = i0 - 4, oy = j0 - 1;
+    const bool in = i < nx && j < ny;
+    const bool ring = i == 0 || i == nx - 1 || j == 0 || j == ny - 1;
+    // this thread's chunks of one level: plane p (species 0..n-1, U, V), row, chunk
+    const float *src[NCH];
+    size_t off[NCH];
+    int dst[NCH];
+    bool ok[NCH];
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        const int e = threadIdx.x + c * NT;
+        dst[c] = -1;
+        ok[c] = false;
+        off[c] = 0;
+        src[c] = U;
+        if (e < NPL * CPR * PH) {
+            const int p = e / (CPR * PH), r = e % (CPR * PH);
+            const int ly = r / CPR, cx = r % CPR;
+            const bool use = p < n || p >= SGMAX;
+            if (use) {
+                const int gi = ox + 4 * cx, gj = oy + ly;
+                const bool yface = p == SGMAX + 1;
+                dst[c] = p * PLANE + ly * PW + 4 * cx;
+                src[c] = p < SGMAX ? sp.q0[s0 + p] : (yface ? V : U);
+                ok[c] = gi >= 0 && gi < g.P && gj >= 0 && gj < (yface ? ny + 1 : ny);
+                if (ok[c]) off[c] = (size_t)gi + (size_t)g.P * nz * gj;
+            }
+        }
+    }
+    auto issue = [&](int k) {
+        if (k < nz) {
+            float *slot = sm + (size_t)(k % NSL) * NPL * PLANE;
+            const size_t lo = (size_t)k * g.P;
+#pragma unroll
+            for (int c = 0; c < NCH; c++)
+                if (dst[c] >= 0) cp_async16(slot + dst[c], ok[c] ? src[c] + off[c] + lo : src[c], ok[c]);
+        }
+        cp_async_commit();
+    };
+    issue(0);
+    issue(1);
+    issue(2);
+    const int pc = (j - oy) * PW + (i - ox);
+    const size_t c0 = in ? ix(g, i, 0, j) : 0, sz = (size_t)g.P;
+    float wb = 0.0f;  // W_m one level down
+    float n_wt = in ? W[c0] : 0.0f, n_G = in ? Gc[c0] : 0.0f, n_djr = in ? DJR[c0] : 0.0f;
+    for (int k = 0; k < nz; k++) {
+        cp_async_wait<1>();   // levels up to k+1 have landed
+        __syncthreads();      // and every thread is done with level k-1
+        issue(k + 3);         // into the slot of level k-2
+        const float wt = n_wt, G = n_G, djr = n_djr;
+        if (in && k + 1 < nz) {
+            n_wt = W[c0 + (k + 1) * sz];
+            n_G = Gc[c0 + (k + 1) * sz];
+            n_djr = DJR[c0 + (k + 1) * sz];
+        }
+        if (!in) continue;
+        const float *L = sm + (size_t)(k % NSL) * NPL * PLANE;
+        const float *Lu = sm + (size_t)((k + 1) % NSL) * NPL * PLANE;
+        const float *Ld = sm + (size_t)((k + NSL - 1) % NSL) * NPL * PLANE;
+        const size_t c = c0 + k * sz;
+        if (ring) {
+            for (int u = 0; u < n; u++) {
+                const float q0 = L[u * PLANE + pc];
+                sp.q1[s0 + u][c] = q0;
+                sp.out[s0 + u][c] = q0;
+            }
+        } else {
+            const float ue = L[SGMAX * PLANE + pc + 1], uw = L[SGMAX * PLANE + pc];
+            const float vn = L[(SGMAX + 1) * PLANE + pc + PW], vs = L[(SGMAX + 1) * PLANE + pc];
+            const bool mid = k > 0 && k < nz - 1;
+            for (int u = 0; u < n; u++) {
+                const float *Q = L + u * PLANE + pc;
+                const float q0 = Q[0];
+                const float fe = flux1(q0, Q[1], ue);
+                const float fw = flux1(Q[-1], q0, uw);
+                const float f3 = flux1(q0, Q[PW], vn);
+                const float f4 = flux1(Q[-PW], q0, vs);
+                float val = q0 - ((fe - fw) + (f3 - f4)) / G;
+                if (mid) {
+                    const float f5t = flux1(q0, Lu[u * PLANE + pc], wt);
+                    const float f5b = flux1(Ld[u * PLANE + pc], q0, wb);
+                    val = val - (f5t - f5b) / djr;
+                } else if (k == 0) {
+                    const float f5t = flux1(q0, Lu[u * PLANE + pc], wt);
+                    val = val - f5t / djr;
+                } else {
+                    const float f5b = flux1(Ld[u * PLANE + pc], q0, wb);
+                    val = val - (q0 * wt - f5b) / djr;
+                }
+                sp.q1[s0 + u][c] = val;
+            }
+        }
+        wb = wt;
+    }
+    cp_async_wait<0>();
+}
+
+
 // Beta of the FCT limiter, num/den with den > 0 and num >= 0.  Only
 // min(1, beta) is ever used, so a quotient >= 1 is returned as 1 without
 // dividing (num >= den implies RN(num/den) >= 1), and num == 0 gives +0
@@ -718,7 +849,9 @@ inline cudaError_t mp_corr_attr()
 // Allow every instantiation its dynamic shared memory (once per device).
 inline cudaError_t mp_corr_setup()
 {
-    cudaError_t e = mp_corr_attr<MpShape8>();
+    cudaError_t e = cudaFuncSetAttribute(k_mp_upwind_cols, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)upf::SMEM);
+    if (e == cudaSuccess) e = mp_corr_attr<MpShape8>();
     if (e == cudaSuccess) e = mp_corr_attr<MpShape16>();
     if (e == cudaSuccess) e = mp_corr_attr<MpShape24>();
     if (e == cudaSuccess) e = mp_corr_attr<MpShape32>();
