@@ -3,7 +3,8 @@
 // launches whatever the number of members, captured once in a CUDA graph:
 //   k_batch_forcing  relaxation-zone update of every forced species
 //   k_batch_prep     species-independent per-step fields of every member
-//   k_batch_upwind   donor-cell pass of every species of every member
+//   k_batch_upwind   donor-cell pass of every species of every member (a
+//                    column march over shared-memory level planes per tile)
 //   (counter reset)
 //   k_batch_corr     persistent CTAs pulling (member, species, tile) items
 //                    from a cost-sorted work list with an atomic counter and
@@ -127,24 +128,30 @@ __global__ void k_batch_prep(const BatchMember *__restrict__ mem, const int *__r
     }
 }
 
-// prefix over members of upwind_ngroups(S, sg) * ceil(nx*nz*ny/256) blocks:
-// each thread takes one species group of one cell
-__global__ void k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix, int nmem, int sg)
+// Donor-cell pass of every member: prefix over members of
+// upwind_cols_blocks(g, S, sg) blocks, each one 32 x 8 column tile of one
+// species group (upwind_cols_tile of mpdata_fused.cuh).
+__host__ __device__ inline int upwind_cols_group(int S, int sg) { return min(upwind_group(S, sg), upf::SGMAX); }
+__host__ __device__ inline int upwind_cols_blocks(const Geo &g, int S, int sg)
 {
+    const int grp = upwind_cols_group(S, sg);
+    const int ng = grp > 0 ? (S + grp - 1) / grp : 0;
+    return ng * ((g.nx + upf::BX - 1) / upf::BX) * ((g.ny + upf::BY - 1) / upf::BY);
+}
+
+__global__ void __launch_bounds__(upf::NT)
+    k_batch_upwind(const BatchMember *__restrict__ mem, const int *__restrict__ prefix, int nmem, int sg)
+{
+    extern __shared__ float4 sm4[];
     const int mi = find_owner(prefix, nmem, blockIdx.x);
     const BatchMember &m = mem[mi];
     const Geo g = m.g;
-    const int grp = upwind_group(m.S, sg);
-    const int nblk = (int)(((size_t)g.nx * g.nz * g.ny + 255) / 256);
+    const int grp = upwind_cols_group(m.S, sg);
+    const int tx = (g.nx + upf::BX - 1) / upf::BX, ty = (g.ny + upf::BY - 1) / upf::BY;
     const int local = blockIdx.x - prefix[mi];
-    const int s0 = (local / nblk) * grp;
-    const size_t t = (size_t)(local % nblk) * blockDim.x + threadIdx.x;
-    const int i = (int)(t % (size_t)g.nx);
-    const size_t rest = t / (size_t)g.nx;
-    const int k = (int)(rest % (size_t)g.nz);
-    const int j = (int)(rest / (size_t)g.nz);
-    if (j >= g.ny) return;
-    mp_upwind_at(g, i, k, j, m.q0 + s0, m.q1 + s0, m.out + s0, min(grp, m.S - s0), m.Um, m.Vm, m.Wm, m.Gc, m.DJR);
+    const int s0 = (local / (tx * ty)) * grp, tile = local % (tx * ty);
+    upwind_cols_tile(reinterpret_cast<float *>(sm4), g, m.q0 + s0, m.q1 + s0, m.out + s0, min(grp, m.S - s0),
+                     (tile % tx) * upf::BX, (tile / tx) * upf::BY, m.Um, m.Vm, m.Wm, m.Gc, m.DJR);
 }
 
 // Persistent correction kernel: items are (member, species, i0, j0).
@@ -182,7 +189,8 @@ inline cudaError_t batch_corr_attr()
 
 inline cudaError_t batch_setup()
 {
-    cudaError_t e = batch_corr_attr<MpShape8>();
+    cudaError_t e = cudaFuncSetAttribute(k_batch_upwind, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upf::SMEM);
+    if (e == cudaSuccess) e = batch_corr_attr<MpShape8>();
     if (e == cudaSuccess) e = batch_corr_attr<MpShape16>();
     if (e == cudaSuccess) e = batch_corr_attr<MpShape24>();
     if (e == cudaSuccess) e = batch_corr_attr<MpShape32>();

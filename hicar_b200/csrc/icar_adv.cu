@@ -1626,9 +1626,8 @@ int build_tables(icar_adv_batch_t *b)
         fill_member(mem[1][m], h, b->dts[m], b->parity == 0 ? 1 : 0);
         const Geo &g = h->g;
         const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
-        const size_t nc = (size_t)g.nx * g.nz * g.ny;
         prep[m + 1] = prep[m] + (int)((nf + 255) / 256);
-        up[m + 1] = up[m] + icar::upwind_ngroups(h->desc.n_species, b->sp_group) * (int)((nc + 255) / 256);
+        up[m + 1] = up[m] + icar::upwind_cols_blocks(h->g, h->desc.n_species, b->sp_group);
         for (int s = 0; s < h->desc.n_species; s++) {
             if (h->forcing[s].p && h->nzone > 0) {
                 pairs.push_back(make_int2(m, s));
@@ -1721,7 +1720,8 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
         icar::k_batch_forcing<<<b->n_force, 256, 0, st>>>(mem, b->d_ints + b->off_f, b->d_pairs, b->n_pairs);
     if (b->n_prep > 0) icar::k_batch_prep<<<b->n_prep, 256, 0, st>>>(mem, b->d_ints, M);
     if (b->n_up > 0)
-        icar::k_batch_upwind<<<b->n_up, 256, 0, st>>>(mem, b->d_ints + b->off_up, M, b->sp_group);
+        icar::k_batch_upwind<<<b->n_up, icar::upf::NT, icar::upf::SMEM, st>>>(mem, b->d_ints + b->off_up, M,
+                                                                           b->sp_group);
     cudaMemsetAsync(b->d_ints + b->off_counter, 0, sizeof(int), st);
     if (b->n_items > 0)
         icar::batch_corr_launch(st, b->shape, b->ctas, b->fct, mem, b->d_items, b->n_items,

@@ -217,17 +217,16 @@ constexpr int NCH = (NPL * CPR * PH + NT - 1) / NT;
 constexpr size_t SMEM = (size_t)NSL * NPL * PLANE * sizeof(float);
 }  // namespace upf
 
-__global__ void __launch_bounds__(upf::NT)
-    k_mp_upwind_cols(Geo g, const __grid_constant__ SpeciesPtrs sp, int S, int sg, const float *__restrict__ U,
-                     const float *__restrict__ V, const float *__restrict__ W, const float *__restrict__ Gc,
-                     const float *__restrict__ DJR)
+// One 32 x 8 column tile (first column i0, first row j0) for species
+// q0s[0..n), n <= upf::SGMAX; sm is the CTA's dynamic shared memory.
+__device__ __forceinline__ void upwind_cols_tile(float *sm, const Geo &g, const float *const *q0s, float *const *q1s,
+                                                 float *const *outs, int n, int i0, int j0,
+                                                 const float *__restrict__ U, const float *__restrict__ V,
+                                                 const float *__restrict__ W, const float *__restrict__ Gc,
+                                                 const float *__restrict__ DJR)
 {
     using namespace upf;
-    extern __shared__ float4 sm4[];
-    float *sm = reinterpret_cast<float *>(sm4);
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
-    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
-    const int s0 = blockIdx.z * sg, n = min(sg, S - s0);
     const int i = i0 + tx, j = j0 + ty;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int ox = i0 - 4, oy = j0 - 1;
@@ -253,7 +252,7 @@ __global__ void __launch_bounds__(upf::NT)
                 const int gi = ox + 4 * cx, gj = oy + ly;
                 const bool yface = p == SGMAX + 1;
                 dst[c] = p * PLANE + ly * PW + 4 * cx;
-                src[c] = p < SGMAX ? sp.q0[s0 + p] : (yface ? V : U);
+                src[c] = p < SGMAX ? q0s[p] : (yface ? V : U);
                 ok[c] = gi >= 0 && gi < g.P && gj >= 0 && gj < (yface ? ny + 1 : ny);
                 if (ok[c]) off[c] = (size_t)gi + (size_t)g.P * nz * gj;
             }
@@ -294,8 +293,8 @@ __global__ void __launch_bounds__(upf::NT)
         if (ring) {
             for (int u = 0; u < n; u++) {
                 const float q0 = L[u * PLANE + pc];
-                sp.q1[s0 + u][c] = q0;
-                sp.out[s0 + u][c] = q0;
+                q1s[u][c] = q0;
+                outs[u][c] = q0;
             }
         } else {
             const float ue = L[SGMAX * PLANE + pc + 1], uw = L[SGMAX * PLANE + pc];
@@ -320,12 +319,23 @@ __global__ void __launch_bounds__(upf::NT)
                     const float f5b = flux1(Ld[u * PLANE + pc], q0, wb);
                     val = val - (q0 * wt - f5b) / djr;
                 }
-                sp.q1[s0 + u][c] = val;
+                q1s[u][c] = val;
             }
         }
         wb = wt;
     }
     cp_async_wait<0>();
+}
+
+__global__ void __launch_bounds__(upf::NT)
+    k_mp_upwind_cols(Geo g, const __grid_constant__ SpeciesPtrs sp, int S, int sg, const float *__restrict__ U,
+                     const float *__restrict__ V, const float *__restrict__ W, const float *__restrict__ Gc,
+                     const float *__restrict__ DJR)
+{
+    extern __shared__ float4 sm4[];
+    const int s0 = blockIdx.z * sg;
+    upwind_cols_tile(reinterpret_cast<float *>(sm4), g, sp.q0 + s0, sp.q1 + s0, sp.out + s0, min(sg, S - s0),
+                     blockIdx.x * upf::BX, blockIdx.y * upf::BY, U, V, W, Gc, DJR);
 }
 
 
