@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--serve-steps-scale", type=float, default=0.1)
     p.add_argument("--members", type=int, default=64, help="ensemble size (ensemble workload)")
     p.add_argument("--tile-shape", default="auto", choices=["auto", "0", "1", "2", "3"],
-                   help="fused-kernel tile shape 0..3 (8/16/24/32 rows), or auto: chosen by hicar_b200.autotune")
+                   help="fused-kernel tile shape 0..3 (8/15/24/31 rows), or auto: chosen by hicar_b200.autotune")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
     p.add_argument("--quick", action="store_true",

@@ -302,7 +302,7 @@ class Domain:
         return int(b.value)
 
     def set_launch_shape(self, tile_shape: int | None = None, species_group: int | None = None) -> None:
-        """Tile shape of the fused correction kernel (0..3 = 8/16/24/32 rows
+        """Tile shape of the fused correction kernel (0..3 = 8/15/24/31 rows
         per tile) and species per thread of its donor-cell pass (0 = all);
         see hicar_b200.autotune.  Results do not depend on either."""
         lib = L.load()

@@ -3,8 +3,8 @@
 Two knobs, neither of which changes any result (every combination gives
 bit-identical fields; tests/test_autotune_gpu.py checks it):
 
-  tile shape     output rows per tile of the correction kernel (8, 16, 24 or
-                 32 rows of 28 columns).  Taller tiles recompute less of the
+  tile shape     output rows per tile of the correction kernel (8, 15, 24 or
+                 31 rows of 28 columns).  Taller tiles recompute less of the
                  y halo around each tile but need more shared memory per CTA,
                  so fewer CTAs fit on an SM, and waste more rows in the last
                  tile of a column when ny-2 is not a multiple of the height.
@@ -34,7 +34,7 @@ from dataclasses import asdict, dataclass
 from pathlib import Path
 
 TILE_COLUMNS = 28
-TILE_ROWS = (8, 16, 24, 32)          # icar_adv_tile_shapes order
+TILE_ROWS = (8, 15, 24, 31)          # icar_adv_tile_shapes order
 _mem_cache: dict[str, dict] = {}
 
 

@@ -171,8 +171,12 @@ struct Shape {
     static constexpr int NT = 32 * NW_;
     static constexpr int PH = TY_ + 4;
     static constexpr int PLANE = PW * PH;
-    static constexpr int RPW = TY_ / NW_;
-    static_assert(TY_ % NW_ == 0, "rows per warp must be whole");
+    static constexpr int RPW = (TY_ + NW_ - 1) / NW_;
+    // one warp beyond the output rows (NW = TY+1): it owns no output row and
+    // takes the face and limiter rows a tile has beyond TY, so every warp
+    // does the same number of rows per level
+    static constexpr bool EXTRA = NW_ == TY_ + 1;
+    static_assert(TY_ % NW_ == 0 || EXTRA, "rows per warp must be whole");
 };
 // shared-memory plane slots
 constexpr int S_Q1 = 0;           // 4 ring slots: level l -> S_Q1 + (l & 3)
@@ -517,7 +521,8 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                 }
                 AT(S_U2, lx, ly) = u2;
             }
-            for (int r = warp; r < TY + 3; r += NW) {  // v2 faces y in [-1, TY+1] -> ly 1..TY+3
+            for (int r = SH::EXTRA && warp == TY ? TY : warp; r < (!SH::EXTRA ? TY + 3 : warp == TY ? TY + 3 : warp + 1);
+                 r += SH::EXTRA ? 1 : NW) {  // v2 faces y in [-1, TY+1] -> ly 1..TY+3
                 const int ly = r + 1, lx = lane;
                 const int i = i0 - 2 + lx, gf = j0 - 2 + ly;
                 float v2 = 0.0f;
@@ -554,7 +559,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
                 float w2 = 0.0f, fz = 0.0f;
                 const int iw = i0 - 2 + lx, jw = j0 - 2 + ly;
-                if (lane < TX && t < nz - 1 && iw >= 1 && iw <= nx - 2 && jw <= ny - 2) {
+                if (warp + NW * rr < TY && lane < TX && t < nz - 1 && iw >= 1 && iw <= nx - 2 && jw <= ny - 2) {
                     const float rq = AT(sQp, lx, ly), lq = AT(sQc, lx, ly);
                     const float ww = AT(sWc, lx, ly);
                     const float Gs = AT(sGp, lx, ly) + AT(sGc, lx, ly);
@@ -617,7 +622,9 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                         AT(S_BXO, lx, ly) = fct_beta(qc - qmin, fout + e15);
                     }
                 }
-                for (int r = warp; r < TY + 2; r += NW) {  // y: cells y in [-1, TY] -> ly 1..TY+2
+                for (int r = SH::EXTRA && warp == TY ? TY : warp;
+                     r < (!SH::EXTRA ? TY + 2 : warp == TY ? TY + 2 : warp + 1);
+                     r += SH::EXTRA ? 1 : NW) {  // y: cells y in [-1, TY] -> ly 1..TY+2
                     const int ly = r + 1, lx = lane;
                     const int j = j0 - 2 + ly;
                     if (lx >= 2 && lx < TX + 2 && j <= ny - 1) {
@@ -651,7 +658,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                 for (int rr = 0; rr < RPW; rr++) {  // z: the output cell at level t
                     const int ly = warp + NW * rr + 2, lx = lane + 2;
                     float bzi = 0.0f, bzo = 0.0f;
-                    if (lane < TX) {
+                    if (warp + NW * rr < TY && lane < TX) {
                         float qmax, qmin, fin, fout;
                         const float qc = AT(sQc, lx, ly), q0c = AT(sQ0c, lx, ly);
                         if (t == 0) {
@@ -689,7 +696,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
                 const int i = i0 - 2 + lx, j = j0 - 2 + ly;
                 n_part[rr] = 0.0f;
-                if (lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
+                if (warp + NW * rr < TY && lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
                     float uw = AT(S_U2, lx, ly), ue = AT(S_U2, lx + 1, ly);
                     float vs = AT(S_V2, lx, ly), vn = AT(S_V2, lx, ly + 1);
                     if (FCT) {
@@ -727,7 +734,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
             for (int rr = 0; rr < RPW; rr++) {
                 const int ly = warp + NW * rr + 2, lx = lane + 2;
                 const int i = i0 - 2 + lx, j = j0 - 2 + ly;
-                if (lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
+                if (warp + NW * rr < TY && lane < TX && i >= 1 && i <= nx - 2 && j <= ny - 2) {
                     const float qc = r_q1dn[rr];
                     const float wtop = n_w2l[rr], wbot = r_w2l[rr];
                     float val = r_part[rr];
@@ -835,13 +842,13 @@ namespace icar {
 // Tile shapes of the fused correction kernel (selected per grid shape by
 // the autotuner): output rows per tile and warps per CTA.
 using MpShape8 = mpf::Shape<8, 4>;
-using MpShape16 = mpf::Shape<16, 16>;
+using MpShape16 = mpf::Shape<15, 16>;
 using MpShape24 = mpf::Shape<24, 8>;
-using MpShape32 = mpf::Shape<32, 32>;
+using MpShape32 = mpf::Shape<31, 32>;
 constexpr int MP_NSHAPES = 4;
 inline int mp_shape_ty(int shape)
 {
-    const int ty[MP_NSHAPES] = {8, 16, 24, 32};
+    const int ty[MP_NSHAPES] = {8, 15, 24, 31};
     return ty[shape < 0 || shape >= MP_NSHAPES ? 1 : shape];
 }
 

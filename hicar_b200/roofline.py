@@ -55,8 +55,8 @@ def species_pass(nx: int, ny: int, nz: int, S: int, total_ms: float, passes: int
 
 # DRAM bytes (read + write) per cell-species of one k_mp_corr launch, from
 # the ncu capture summarised in profiles/k_mp_corr_256x256x40x12.md
-# (256x256x40, 12 species, tile shape 16 rows, FCT on).
-CORR_DRAM_BYTES_PER_CS = 13.88
+# (256x256x40, 12 species, tile shape 1, FCT on).
+CORR_DRAM_BYTES_PER_CS = 13.87
 
 
 def correction_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launches: int) -> dict:

@@ -30,8 +30,8 @@ def test_batch_shape_model_prefers_less_waste():
     # per row unless their last tile is mostly empty
     costs = {s: r + 4.0 for s, r in enumerate(A.TILE_ROWS)}
     assert A.choose_batch_shape([(64, 10, 20, 12)], costs) == 0       # 8 interior rows: one 8-row tile
-    assert A.choose_batch_shape([(64, 34, 20, 12)], costs) == 3       # 32 rows: one 32-row tile, no waste
-    assert A.choose_batch_shape([(64, 10, 20, 12)] * 3 + [(64, 34, 20, 12)], costs) == 0
+    assert A.choose_batch_shape([(64, 33, 20, 12)], costs) == 3       # 31 rows: one 31-row tile, no waste
+    assert A.choose_batch_shape([(64, 10, 20, 12)] * 3 + [(64, 33, 20, 12)], costs) == 0
     # a shape that is cheaper per row wins when waste is equal
     costs2 = {0: 8.0, 1: 14.0, 2: 24.0, 3: 32.0}
     assert A.choose_batch_shape([(300, 258, 40, 12)], costs2) == 1

@@ -186,7 +186,7 @@ def test_closed_domain_mass_gpu(oracle_lib):
 
 @pytest.mark.parametrize("nx,ny,nz", [(3, 3, 3), (30, 18, 3), (29, 17, 5), (57, 33, 7), (100, 70, 41), (31, 200, 4)])
 def test_fused_matches_oracle_on_ragged_shapes(oracle_lib, nx, ny, nz):
-    """Tile edges of the fused kernel (28x16 column tiles) at every offset,
+    """Tile edges of the fused kernel (28-column tiles) at every offset,
     the smallest legal domain and short/tall columns."""
     O = oracle_lib
     case = synth.config2(seed=nx + ny + nz, nx=nx, ny=ny, nz=nz)
