@@ -432,7 +432,7 @@ def run_large(args):
                                         "chosen_by": "autotune: every combination timed on this domain"},
                        "l2": "inputs larger than L2 (12 fields x 1 GB)"},
             "plain": {"value": cs * args.steps / (ms_plain / 1e3), "ms_per_step": ms_plain / args.steps,
-                      "launch_shape": {"tile_rows": 16, "species_group": 0}},
+                      "launch_shape": {"tile_rows": autotune.TILE_ROWS[1], "species_group": 0}},
             "autotuned_over_plain": ms_plain / ms,
             "autotune_ms_per_step": measured,
             "device_bytes": d.device_bytes(),
