@@ -151,13 +151,8 @@ __global__ void k_mp_upwind(Geo g, const __grid_constant__ SpeciesPtrs sp, int S
     mp_upwind_at(g, i, k, j, sp.q0 + s0, sp.q1 + s0, sp.out + s0, min(sg, S - s0), U, V, W, Gc, DJR);
 }
 
-// Blocks of the species dimension for a species group (0 = all species).
+// Species per group of the donor-cell pass for the knob sg (0 = all species).
 __host__ __device__ inline int upwind_group(int S, int sg) { return sg <= 0 || sg > S ? S : sg; }
-__host__ __device__ inline int upwind_ngroups(int S, int sg)
-{
-    const int g = upwind_group(S, sg);
-    return g > 0 ? (S + g - 1) / g : 0;
-}
 
 namespace mpf {
 constexpr int TX = 28;            // output columns per tile

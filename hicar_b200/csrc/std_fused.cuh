@@ -137,7 +137,6 @@ struct Shape {
     static constexpr int NT = 32 * NW_;
     static constexpr int TX = CORR_ ? 28 : 32;
     static constexpr int HX = CORR_ ? 4 : 3;         // plane halo
-    static constexpr int OWN = CORR_ ? 2 : 0;        // owned columns/rows start OWN before the tile
     static constexpr int RY = CORR_ ? TY_ + 4 : TY_; // owned rows
     static constexpr int RPW = RY / NW_;
     static constexpr int PW = CORR_ ? 40 : 44;
