@@ -14,8 +14,10 @@
 // single upward sweep: each level's downward flux is formed from the level
 // above before that level is touched, exactly the reference's values and
 // order) with the evaporation/sublimation of what fell into unsaturated
-// levels.  Phase 4 turns T back into th.  The column's rain and snow are
-// added to the real64 accumulations (one writer per column).
+// levels.  Phase 4 turns T back into th.  With one substep each (the usual
+// case) phases 2-4 run as a second staged march, level by level (see the
+// kernel).  The column's rain and snow are added to the real64
+// accumulations (one writer per column).
 //
 // Arithmetic follows the reference expression by expression (no FMA
 // contraction).  The one transcendental, exp in sat_mr, is evaluated as the
@@ -183,12 +185,13 @@ __global__ void __launch_bounds__(mpsf::NT)
     int stop = 0;
     const float *src[NCH];
     size_t off[NCH];
-    int dst[NCH];
+    int dst[NCH], fld[NCH];
     bool ok[NCH];
 #pragma unroll
     for (int c = 0; c < NCH; c++) {
         const int e = threadIdx.x + c * NT;
         dst[c] = -1;
+        fld[c] = 0;
         ok[c] = false;
         off[c] = 0;
         src[c] = pressure;
@@ -197,6 +200,8 @@ __global__ void __launch_bounds__(mpsf::NT)
             const int ly = r / CPR, cx = r % CPR;
             const int gi = ox + 4 * cx, gj = oy + ly;
             dst[c] = f * PLANE + ly * PW + 4 * cx;
+            fld[c] = f;
+            // phase 1 planes: pressure, th, pii, qv, qc, qr, qs, dz
             src[c] = f == 0 ? pressure : f == 1 ? th : f == 2 ? pii : f == 3 ? qv : f == 4 ? qc : f == 5 ? qr : f == 6 ? qs : dz;
             ok[c] = gi < g.P && gj < g.ny;
             if (ok[c]) off[c] = (size_t)gi + (size_t)g.P * nz * gj;
@@ -248,7 +253,121 @@ __global__ void __launch_bounds__(mpsf::NT)
         qs[c] = s;
     }
     cp_async_wait<0>();
+    __syncthreads();  // phase 1's results are in global memory for the planes below
+
+    // Sedimentation parameters (the reference's expressions).  A column
+    // whose rain and snow each take at most one substep runs phases 2-4 as
+    // one more upward march over staged planes: at level k the rain and
+    // snow sweeps finalise that level (each level's downward flux comes from
+    // the level above), then rain evaporates and snow sublimates there and
+    // th = T/pii is formed.  Every operation at level k reads and writes
+    // level k only, apart from the sweeps' carried values, so the values
+    // and their order are those of the separate passes.  Columns with more
+    // substeps take the passes below.
+    float fr_r = 0.0f, rate_r = 0.0f, fr_s = 0.0f, rate_s = 0.0f;
+    int ns_r = 0, ns_s = 0;
+    if (col && mx_r > mps::SMALL) {
+        const float cfl = ceilf(m_r);
+        fr_r = dt * mps::RAIN_FALL / cfl;
+        ns_r = (int)lrintf(cfl);
+        rate_r = cloud2rain / (float)(2 * ns_r);
+    }
+    if (col && mx_s > mps::SMALL) {
+        const float cfl = ceilf(m_s);
+        fr_s = dt * mps::SNOW_FALL / cfl;
+        ns_s = (int)lrintf(cfl);
+        rate_s = cloud2snow / (float)(2 * ns_s);
+    }
+    const bool fused = col && ns_r <= 1 && ns_s <= 1;
+    // march 2 planes: th (T), qv, pressure, pii, qr, qs, rho, dz
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+        const int f = fld[c];
+        src[c] = f == 0 ? th : f == 1 ? qv : f == 2 ? pressure : f == 3 ? pii : f == 4 ? qr : f == 5 ? qs : f == 6 ? rho : dz;
+    }
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) issue(k);
+    float qi_r = 0.0f, qi_s = 0.0f, sed_r = 0.0f, sed_s = 0.0f;
+    for (int k = 0; k < nz; k++) {
+        cp_async_wait<DEPTH - 2>();  // levels k and k+1 have landed
+        __syncthreads();
+        issue(k + DEPTH);            // into the slot of level k-1
+        if (!fused) continue;
+        const float *L = sm + (size_t)(k % NSLOT) * NF * PLANE + pc;
+        const float *Lu = sm + (size_t)((k + 1) % NSLOT) * NF * PLANE + pc;
+        const size_t c = c0 + k * st;
+        if (k == 0) {
+            // sediment out of the bottom level
+            if (ns_r == 1) {
+                qi_r = L[4 * PLANE];
+                sed_r = fr_r * qi_r * L[6 * PLANE];
+                qi_r = qi_r - (sed_r / L[7 * PLANE] / L[6 * PLANE]);
+            }
+            if (ns_s == 1) {
+                qi_s = L[5 * PLANE];
+                sed_s = fr_s * qi_s * L[6 * PLANE];
+                qi_s = qi_s - (sed_s / L[7 * PLANE] / L[6 * PLANE]);
+            }
+        }
+        float r = L[4 * PLANE], sn = L[5 * PLANE];
+        if (ns_r == 1) {
+            if (k < nz - 1) {
+                float qu = Lu[4 * PLANE];
+                const float ru = Lu[6 * PLANE];
+                const float flux = fr_r * qu * ru;
+                qi_r = qi_r + flux / (L[6 * PLANE] * L[7 * PLANE]);
+                qu = qu - flux / (ru * Lu[7 * PLANE]);
+                r = qi_r;
+                qi_r = qu;
+            } else {
+                r = qi_r;
+            }
+        }
+        if (ns_s == 1) {
+            if (k < nz - 1) {
+                float qu = Lu[5 * PLANE];
+                const float ru = Lu[6 * PLANE];
+                const float flux = fr_s * qu * ru;
+                qi_s = qi_s + flux / (L[6 * PLANE] * L[7 * PLANE]);
+                qu = qu - flux / (ru * Lu[7 * PLANE]);
+                sn = qi_s;
+                qi_s = qu;
+            } else {
+                sn = qi_s;
+            }
+        }
+        float T = L[0], v = L[PLANE];
+        const float p = L[2 * PLANE];
+        if (ns_r == 1 && r > mps::SMALL) {
+            const float L_evap = -1.0f * (mps::LH_VAPOR + (373.15f - T) * mps::DLHVDT);
+            const float qvsat = mp_sat_mr(T, p);
+            if (v < qvsat) mp_phase_change(T, r, qvsat, v, L_evap, rate_r, stop);
+        }
+        if (ns_s == 1 && sn > mps::SMALL) {
+            const float L_evap = -1.0f * (mps::LH_VAPOR + (373.15f - T) * mps::DLHVDT);
+            const float qvsat = mp_sat_mr(T, p);
+            if (v < qvsat) mp_phase_change(T, sn, qvsat, v, -1.0f * mps::LH_LIQUID + L_evap, rate_s, stop);
+        }
+        th[c] = T / L[3 * PLANE];
+        qv[c] = v;
+        qr[c] = r;
+        qs[c] = sn;
+    }
+    cp_async_wait<0>();
     if (!col) return;
+    if (fused) {
+        float rain = 0.0f, snow = 0.0f;
+        if (ns_r == 1) rain = rain + sed_r;
+        if (ns_s == 1) {
+            snow = snow + sed_s;
+            rain = rain + sed_s;
+        }
+        const size_t c2 = (size_t)i + (size_t)g.nx * j;
+        acc_rain[c2] = acc_rain[c2] + (double)rain;
+        acc_snow[c2] = acc_snow[c2] + (double)snow;
+        if (stop) atomicOr(stop_flag, 1);
+        return;
+    }
     float rain = 0.0f, snow = 0.0f;
     // phases 2 and 3: sedimentation of rain, then of snow
     for (int pass = 0; pass < 2; pass++) {

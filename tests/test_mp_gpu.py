@@ -61,6 +61,32 @@ def test_mp_simple_matches_oracle(oracle_lib, shape):
         assert rain.sum() > 0          # the deeper cases exercise sedimentation
 
 
+@pytest.mark.parametrize("layout", ["thin", "mixed"])
+def test_mp_simple_several_substeps(oracle_lib, layout):
+    """Thin levels make the sedimentation take several CFL substeps: those
+    columns run the separate passes, the rest the single fused march; with
+    "mixed" both kinds sit side by side in every CTA row."""
+    O = oracle_lib
+    c = mp_case(seed=13, nx=61, ny=47, nz=20)
+    dzm = c.dz_mass.copy()
+    if layout == "thin":
+        dzm *= np.float32(0.05)                       # rain and snow both need several substeps
+    else:
+        dzm[:, :, ::3] *= np.float32(0.1)            # every third column: rain in several substeps
+    c.dz_mass = dzm.astype(np.float32)
+    ref, rain, snow, stop = oracle_mp(O, c, 20.0)
+    d = Domain.from_case(c)
+    adv_init(d, OPTS)
+    mp(d, OPTS, 20.0)
+    got = {k: d.fetch(k).copy() for k in FIELDS}
+    grain, gsnow = precipitation(d)
+    d.close()
+    for k in FIELDS:
+        assert np.array_equal(got[k], ref[k]), (k, int((got[k] != ref[k]).sum()))
+    assert np.array_equal(grain, rain) and np.array_equal(gsnow, snow)
+    assert rain.sum() > 0
+
+
 def test_advect_and_mp_steps(oracle_lib):
     """The resident species go through advect -> mp -> advect -> ... on the
     device without a host round trip; five steps stay within 1e-4 of the
