@@ -311,18 +311,20 @@ __device__ __forceinline__ void std_stage_tile(float *sm, const Geo &g, int its,
         const float *V = PL(P_V + (b & 1));
         float *FX = PL(P_FX);
         float *FY = PL(P_FY);
-        // x faces i0..i0+TX of the tile rows, y faces j0..j0+TY of the tile columns
-        for (int e = threadIdx.x; e < (TX + 1) * TY; e += SH::NT) {
-            const int fx = e % (TX + 1), ry = e / (TX + 1);
-            const int px = i0 + fx - ox, py = j0 + ry - oy;
-            const int p = py * PW + px;
-            FX[p] = hflux(HORD, QF + p, 1, U[p] * tf);
-        }
-        for (int e = threadIdx.x; e < TX * (TY + 1); e += SH::NT) {
-            const int cx = e % TX, fy = e / TX;
-            const int px = i0 + cx - ox, py = j0 + fy - oy;
-            const int p = py * PW + px;
-            FY[p] = hflux(HORD, QF + p, PW, V[p] * tf);
+        // x faces i0..i0+TX of the tile rows, then y faces j0..j0+TY of the
+        // tile columns, as one index range: the leftover faces of both sets
+        // share one last partial round instead of one round each.
+        constexpr int NFX = (TX + 1) * TY, NF = NFX + TX * (TY + 1);
+        for (int e = threadIdx.x; e < NF; e += SH::NT) {
+            if (e < NFX) {
+                const int fx = e % (TX + 1), ry = e / (TX + 1);
+                const int p = (j0 + ry - oy) * PW + (i0 + fx - ox);
+                FX[p] = hflux(HORD, QF + p, 1, U[p] * tf);
+            } else {
+                const int cx = (e - NFX) % TX, fy = (e - NFX) / TX;
+                const int p = (j0 + fy - oy) * PW + (i0 + cx - ox);
+                FY[p] = hflux(HORD, QF + p, PW, V[p] * tf);
+            }
         }
         __syncthreads();
 #pragma unroll
