@@ -7,24 +7,35 @@
 namespace icar {
 
 // Relaxation-zone update over the columns whose filter is non-zero (zone[]
-// holds their (i,j) packed as i + nx*j).  dt is the real64 dt%seconds(); the
-// Fortran expression mixes real and real64, so it is evaluated in double and
-// rounded on assignment.  Columns with filter 0 are left alone: the reference
-// adds 0*(forcing-q) there, which leaves q unchanged for finite inputs.
-// Forcing values are advanced only inside the zone, the only place the
-// advected species read them.
+// holds their (i,j) packed as i + nx*j), for every species that has forcing
+// in one launch (thread index = (species slot, level, zone column)).  dt is
+// the real64 dt%seconds(); the Fortran expression mixes real and real64, so
+// it is evaluated in double and rounded on assignment.  Columns with filter
+// 0 are left alone: the reference adds 0*(forcing-q) there, which leaves q
+// unchanged for finite inputs.  Forcing values are advanced only inside the
+// zone, the only place the advected species read them.
+struct ForcingPtrs {
+    float *q[32];
+    float *forcing[32];
+    const float *dqdt[32];
+};
+
 __global__ void k_apply_forcing(Geo g, int nzone, const int *__restrict__ zone,
-                                const float *__restrict__ filter2d, double dt, float *__restrict__ q,
-                                float *__restrict__ forcing, const float *__restrict__ dqdt)
+                                const float *__restrict__ filter2d, double dt, ForcingPtrs fp, int nslots)
 {
-    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (size_t)nzone * g.nz) return;
-    const int z = (int)(t % (size_t)nzone);
-    const int k = (int)(t / (size_t)nzone);
+    const size_t per = (size_t)nzone * g.nz;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per * (size_t)nslots) return;
+    const int s = (int)(t / per);
+    const size_t r = t - (size_t)s * per;
+    const int z = (int)(r % (size_t)nzone);
+    const int k = (int)(r / (size_t)nzone);
+    float *__restrict__ q = fp.q[s];
+    float *__restrict__ forcing = fp.forcing[s];
     const int packed = zone[z];
     const int i = packed % g.nx, j = packed / g.nx;
     const size_t c = ix(g, i, k, j);
-    const float fnew = (float)((double)forcing[c] + (double)dqdt[c] * dt);
+    const float fnew = (float)((double)forcing[c] + (double)fp.dqdt[s][c] * dt);
     forcing[c] = fnew;
     const float flt = filter2d[packed];
     if (flt == 1.0f)

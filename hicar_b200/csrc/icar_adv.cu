@@ -1085,27 +1085,38 @@ int icar_adv_advect(icar_adv_t *h, float dt)
     return advect_impl(h, dt);
 }
 
+// apply_forcing for the species [s0, s1) that have forcing, in one launch.
+static_assert(ICAR_ADV_MAX_SPECIES <= 32, "ForcingPtrs holds 32 species");
+int forcing_range(icar_adv_t *h, double dt_seconds, int s0, int s1)
+{
+    if (h->nzone == 0) return ICAR_ADV_OK;
+    icar::ForcingPtrs fp{};
+    int ns = 0;
+    for (int s = s0; s < s1; s++) {
+        if (!h->forcing[s].p) continue;
+        if (!h->dqdt[s].p) {
+            int e = alloc(h, h->dqdt[s], h->n_cell);  // zero tendency: fixed inflow
+            if (e) return e;
+        }
+        fp.q[ns] = h->q[s].p;
+        fp.forcing[ns] = h->forcing[s].p;
+        fp.dqdt[ns] = h->dqdt[s].p;
+        ns++;
+    }
+    if (ns == 0) return ICAR_ADV_OK;
+    const size_t n = (size_t)h->nzone * h->g.nz * ns;
+    icar::k_apply_forcing<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->g, h->nzone, h->zone_dev, h->filter_dev,
+                                                                      dt_seconds, fp, ns);
+    return check_launch(h, "apply_forcing");
+}
+
 int icar_adv_apply_forcing(icar_adv_t *h, double dt_seconds)
 {
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
     if (h->batch) return fail(h, ICAR_ADV_BAD_ARG, "domain is a batch member: step it with icar_adv_batch_step");
     cudaSetDevice(h->desc.device);
     if (!std::isfinite(dt_seconds)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite");
-    if (h->nzone == 0) return ICAR_ADV_OK;
-    const size_t n = (size_t)h->nzone * h->g.nz;
-    int launched = 0;
-    for (int s = 0; s < h->desc.n_species; s++) {
-        if (!h->forcing[s].p) continue;
-        launched++;
-        if (!h->dqdt[s].p) {
-            int e = alloc(h, h->dqdt[s], h->n_cell);  // zero tendency: fixed inflow
-            if (e) return e;
-        }
-        icar::k_apply_forcing<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->g, h->nzone, h->zone_dev, h->filter_dev,
-                                                                          dt_seconds, h->q[s].p, h->forcing[s].p,
-                                                                          h->dqdt[s].p);
-    }
-    return check_launch(h, "apply_forcing", launched);
+    return forcing_range(h, dt_seconds, 0, h->desc.n_species);
 }
 
 int icar_adv_enforce_limits(icar_adv_t *h)
@@ -1252,26 +1263,6 @@ int icar_adv_set_precipitation(icar_adv_t *h, const double *rain, const double *
 }
 
 namespace {
-
-// apply_forcing for species [s0, s1) (icar_adv_apply_forcing over a range).
-int forcing_range(icar_adv_t *h, double dt_seconds, int s0, int s1)
-{
-    if (h->nzone == 0) return ICAR_ADV_OK;
-    const size_t n = (size_t)h->nzone * h->g.nz;
-    int launched = 0;
-    for (int s = s0; s < s1; s++) {
-        if (!h->forcing[s].p) continue;
-        launched++;
-        if (!h->dqdt[s].p) {
-            int e = alloc(h, h->dqdt[s], h->n_cell);  // zero tendency: fixed inflow
-            if (e) return e;
-        }
-        icar::k_apply_forcing<<<blocks_for(n, 256), 256, 0, h->stream>>>(h->g, h->nzone, h->zone_dev, h->filter_dev,
-                                                                          dt_seconds, h->q[s].p, h->forcing[s].p,
-                                                                          h->dqdt[s].p);
-    }
-    return check_launch(h, "apply_forcing", launched);
-}
 
 // Species groups of icar_adv_step_host: one species per group up to 12 (on
 // config 2 the step then runs within about 10 % of the page-locked copy

@@ -138,6 +138,26 @@ def test_boundary_forcing_step(oracle_lib):
     assert_exact(out, ref)
 
 
+def test_boundary_forcing_several_species(oracle_lib):
+    """One apply_forcing launch covers every forced species, each with its own
+    forcing and tendency; one species is left unforced."""
+    O = oracle_lib
+    case = synth.config2(seed=4, nx=48, ny=40, nz=10)
+    rng = np.random.default_rng(2)
+    forcing = {}
+    for n, k in enumerate(case.species):
+        if k == "qr":
+            continue
+        q = case.species[k]
+        fh = (q * np.float32(1.0 + 0.02 * (n + 1))).astype(np.float32)
+        dq = (rng.standard_normal(q.shape) * 1e-6 * float(np.abs(q).max())).astype(np.float32)
+        forcing[k] = (fh, dq)
+    flt = O.init_relax_filters(case.nx, case.ny, 2)
+    ref = O.run_steps(case, O.make_opts(), case.dt, 6, forcing=forcing, filter2d=flt)
+    out = gpu_run(case, Options(), 6, forcing=forcing)
+    assert_exact(out, ref)
+
+
 def test_relax_filter_matches_oracle(oracle_lib):
     case = synth.config1(seed=1, nx=50, ny=40, nz=6)
     d = Domain.from_case(case)
