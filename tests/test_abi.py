@@ -96,3 +96,22 @@ def test_restart_vars_match_reference_request(cuda_lib):
     assert lib.icar_adv_restart_vars(None, ids, C.byref(n)) == cuda_lib.BAD_ARG
     assert lib.icar_adv_download(None, 0, None, None) == cuda_lib.BAD_ARG
     assert lib.icar_adv_upload(None, 0, None, None) == cuda_lib.BAD_ARG
+
+
+def test_c_consumer_compiles_links_and_runs(cuda_lib, tmp_path):
+    """The header compiles as strict C99 and a C program linked to the
+    library runs its host-only entry points (tests/c_consumer.c), as a
+    Fortran shim bound through ISO_C_BINDING would call them."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    so = Path(cuda_lib.LIB_PATH)
+    exe = tmp_path / "c_consumer"
+    cmd = [gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", str(ROOT / "include"),
+           str(ROOT / "tests" / "c_consumer.c"), "-o", str(exe), str(so), f"-Wl,-rpath,{so.parent}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
