@@ -1,7 +1,7 @@
 """Simple microphysics (SB04, mp_simple.f90) on the GPU against the CPU
 oracle, through the C ABI.  Both evaluate exp in the saturation mixing
 ratio as the correctly rounded single-precision value, so the fields agree
-cell for cell; the north_star tolerance (max relative error <= 1e-5 per
+cell for cell; the path's stated tolerance (max relative error <= 1e-5 per
 call, <= 1e-4 after repeated advect -> mp steps, floor 1e-6 * max|q|) is
 asserted as well, and the real64 precipitation accumulations to the same
 bounds."""

@@ -3,7 +3,7 @@
 Every kernel evaluates the reference's FP32 expressions in the same order
 without fused multiply-adds, so the bar is bit-exact equality with the FP32
 oracle (np.array_equal); the error against the FP64 oracle is reported as
-well.  The north_star tolerance (max relative error <= 1e-5 per step,
+well.  The path's stated tolerance (max relative error <= 1e-5 per step,
 <= 1e-4 after 100 steps) is asserted too, so a deliberate relaxation of the
 arithmetic would still be judged against it.
 """
