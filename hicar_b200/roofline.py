@@ -54,8 +54,8 @@ def species_pass(nx: int, ny: int, nz: int, S: int, total_ms: float, passes: int
 
 
 # DRAM bytes (read + write) per cell-species of one k_mp_corr launch, from
-# the ncu capture summarised in profiles/k_mp_corr_256x256x40x12.md
-# (256x256x40, 12 species, tile shape 1, FCT on).
+# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of a
+# 256x256x40, 12-species launch with tile shape 1 and FCT on.
 CORR_DRAM_BYTES_PER_CS = 13.87
 
 
