@@ -115,3 +115,26 @@ def test_c_consumer_compiles_links_and_runs(cuda_lib, tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
+
+
+def test_standard_scheme_needs_an_updated_column_and_row(cuda_lib):
+    """The standard scheme updates its..ite x jts..jte, the domain less its
+    halo on each side; a domain with no such cell is refused (BAD_ARG)."""
+    lib = cuda_lib.load()
+    o = cuda_lib.Opts()
+    lib.icar_adv_default_opts(C.byref(o))
+    o.advection, o.h_order, o.v_order, o.flux_corr = 1, 5, 3, 1
+    hs = lib.icar_adv_halo_size(C.byref(o))
+    assert hs == 4
+    d = cuda_lib.Desc()
+    d.nx, d.ny, d.nz, d.dx, d.n_species = 2 * hs + 1, 2 * hs + 1, 3, 1000.0, 1
+    d.species[0] = cuda_lib.F_QV
+    b = C.c_int64()
+    assert lib.icar_adv_footprint(C.byref(d), C.byref(o), C.byref(b)) == 0
+    for nx, ny in [(2 * hs, 2 * hs + 1), (2 * hs + 1, 2 * hs)]:
+        d.nx, d.ny = nx, ny
+        assert lib.icar_adv_footprint(C.byref(d), C.byref(o), C.byref(b)) == cuda_lib.BAD_ARG
+        assert b"twice the halo" in lib.icar_adv_last_error(None)
+    o.advection = 2                                  # MPDATA takes any extent >= 3
+    d.nx, d.ny = 3, 3
+    assert lib.icar_adv_footprint(C.byref(d), C.byref(o), C.byref(b)) == 0
