@@ -41,6 +41,54 @@ def test_reference_mpdata_periodic_sine_no_fct(oracle_lib):
     assert np.isfinite(q).all()
 
 
+def _periodic_std_step(O, h, v, fc, rk3, nsteps=400):
+    """The step-function setup of the reference's MPDATA test carried over to
+    the standard scheme, whose update covers the domain less its halo: nx =
+    2*halo + 1 (one updated column), a 1 -> 2 step along 100 updated rows at
+    y Courant 0.25, and the halo rows wrapped periodically after every step.
+    Returns the updated column before and after nsteps (one revolution at
+    400)."""
+    hs = O.halo_size(1, h, v, fc)
+    nyi = 100
+    c = synth.periodic_y_case(ny=nyi + 2 * hs, nx=2 * hs + 1, nz=3, cfl=0.25, step=True)
+    q = np.ones_like(c.species["qv"])
+    q[hs + nyi // 2:hs + nyi] = 2.0
+    c.species = {"qv": q}
+
+    def wrap(a):
+        ny = a.shape[0]
+        a[0:hs] = a[ny - 2 * hs:ny - hs]
+        a[ny - hs:ny] = a[hs:2 * hs]
+
+    wrap(c.species["qv"])
+    q0 = c.species["qv"][hs:-hs, :, hs].copy()
+    o = O.make_opts(advection=1, h_order=h, v_order=v, flux_corr=fc, rk3=rk3)
+    for _ in range(nsteps):
+        c.species = O.advect(c, o, 1.0)
+        wrap(c.species["qv"])
+    return q0, c.species["qv"][hs:-hs, :, hs]
+
+
+@pytest.mark.parametrize("h,v,rk3", [(3, 3, 0), (3, 3, 1), (5, 3, 1), (5, 5, 1)])
+def test_standard_scheme_monotone_with_wrf_correction(oracle_lib, h, v, rk3):
+    """With WRF_flux_corr the step stays inside [1, 2] to FP32 round-off.
+    Without RK3 the mean is kept to round-off; RK3's intermediate stages read
+    the halo rows as they were at the start of the step (the reference
+    exchanges halos once per step, not between stages), so on this wrapped
+    domain the mean drifts by about 1e-4 per revolution."""
+    q0, q = _periodic_std_step(oracle_lib, h, v, 1, rk3)
+    assert q.min() >= 1.0 - 1e-6 and q.max() <= 2.0 + 1e-6
+    drift = abs(q.mean(dtype=np.float64) / q0.mean(dtype=np.float64) - 1.0)
+    assert drift < (1e-6 if not rk3 else 2e-4)
+
+
+def test_standard_scheme_overshoots_without_correction(oracle_lib):
+    """The same fifth-order RK3 step without the correction leaves [1, 2] by
+    several percent: the bounds above are the limiter's doing."""
+    _, q = _periodic_std_step(oracle_lib, 5, 3, 0, 1)
+    assert q.min() < 0.95 and q.max() > 2.05
+
+
 @pytest.mark.parametrize("scheme", ["mpdata", "mpdata_nofct", "upwind", "std1", "std3", "std5", "std5_fc", "std3_rk3"])
 def test_uniform_field_invariance(oracle_lib, scheme):
     """A uniform tracer stays uniform under the divergence-free winds."""
