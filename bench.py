@@ -161,34 +161,46 @@ def cpu_sample(case, rows: int):
 
 def run_reference(args):
     """--impl reference: the oracle port of the reference's CPU advection on
-    this host's cores, on a bounded y-slab sample of the workload per step."""
+    this host's cores, on the same whole domain as the GPU arm (one step of
+    the 512x512x40 x 12-field workload is about 1.4 s on 16 host threads)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     case, desc = make_case(args.workload, 100)
-    rows = 16 if args.workload == "full_species" else case.ny
-    sample = cpu_sample(case, rows)
+    sample = case
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from hicar_b200.build import build_oracle
     build_oracle()
     from oracle import oracle as O
     opts = O.make_opts()
     c = sample
-    for _ in range(args.warmup):
+    # the same step as the GPU arm: fixed-inflow relaxation update
+    # (forcing = initial state, dqdt = 0), then advect
+    flt = O.init_relax_filters(c.nx, c.ny, 2)
+    forcing = {k: (q.copy(), np.zeros_like(q)) for k, q in c.species.items()}
+
+    def one_step():
+        for k, (fh, dq) in forcing.items():
+            O.apply_forcing(c.species[k], fh, dq, flt, c.dt)
         c.species = O.advect(c, opts, c.dt)
+
+    for _ in range(args.warmup):
+        one_step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        c.species = O.advect(c, opts, c.dt)
+        one_step()
     el = time.perf_counter() - t0
     cs = sample.cells() * len(sample.species)
     val = cs * args.steps / el
-    samp = f"{sample.nx}x{sample.ny}x{sample.nz} slab of the {desc.split(',')[0]}, {len(sample.species)} fields"
+    samp = (f"the whole {sample.nx}x{sample.ny}x{sample.nz} domain, {len(sample.species)} fields, every step "
+            f"(C restatement with OpenMP over rows in every stage; the reference threads only the FCT sweep)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": desc, "scheme": "MPDATA order 2 + FCT"},
+        "config": {"workload": desc, "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
+                   "same_config": True},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": samp},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)

@@ -1310,49 +1310,61 @@ int icar_adv_step_host(icar_adv_t *h, double dt_seconds, int32_t enforce_limits,
         h->io_events.assign(2 * IO_GROUPS + 1, nullptr);
         for (auto &ev : h->io_events) CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
-    cudaEvent_t ev_start = h->io_events[2 * IO_GROUPS];
-    // uploads start once the work already queued on the handle's stream is done
-    CUDA_TRY(h, cudaEventRecord(ev_start, h->stream));
-    CUDA_TRY(h, cudaStreamWaitEvent(h->io_in, ev_start, 0));
-    for (int s = 0; s < S; s++) h->have_q[s] = true;
-    if ((e = ensure_ready(h))) return e;
-    const float dt = (float)dt_seconds;
-    if ((e = mp ? mpdata_prep(h, dt) : std_prep(h, dt))) return e;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int64_t before = h->launches;
-    if (h->profiling) {
-        cudaEventCreate(&ev0);
-        cudaEventCreate(&ev1);
-        cudaEventRecord(ev0, h->stream);
-    }
-    auto result = [&](int s) -> DevBuf & { return mp ? h->qn[s] : (h->opts.rk3 ? h->q1s[s] : h->qn[s]); };
-    for (int gi = 0; gi < ngroups; gi++) {
-        const int s0 = S * gi / ngroups, s1 = S * (gi + 1) / ngroups;
-        cudaEvent_t ev_in = h->io_events[gi], ev_done = h->io_events[IO_GROUPS + gi];
-        for (int s = s0; s < s1; s++)
-            if ((e = copy_species_async(h, h->q[s].p, const_cast<float *>(q_in[s]), true, h->io_in))) return e;
-        CUDA_TRY(h, cudaEventRecord(ev_in, h->io_in));
-        CUDA_TRY(h, cudaStreamWaitEvent(h->stream, ev_in, 0));
-        if ((e = forcing_range(h, dt_seconds, s0, s1))) return e;
-        if ((e = mp ? mpdata_group(h, s0, s1) : std_group(h, s0, s1))) return e;
-        if (enforce_limits) {
-            for (int s = s0; s < s1; s++)
-                icar::k_enforce_limits<<<blocks_for(h->n_cell, 256), 256, 0, h->stream>>>(h->g, result(s).p);
-            if ((e = check_launch(h, "enforce_limits", s1 - s0))) return e;
+    // Every return after the first enqueue goes through `pipeline`, so that
+    // on an error the copies already queued into or out of the caller's host
+    // arrays are drained before the call returns.
+    auto pipeline = [&]() -> int {
+        cudaEvent_t ev_start = h->io_events[2 * IO_GROUPS];
+        // uploads start once the work already queued on the handle's stream is done
+        CUDA_TRY(h, cudaEventRecord(ev_start, h->stream));
+        CUDA_TRY(h, cudaStreamWaitEvent(h->io_in, ev_start, 0));
+        for (int s = 0; s < S; s++) h->have_q[s] = true;
+        if ((e = ensure_ready(h))) return e;
+        const float dt = (float)dt_seconds;
+        if ((e = mp ? mpdata_prep(h, dt) : std_prep(h, dt))) return e;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+        int64_t before = h->launches;
+        if (h->profiling) {
+            cudaEventCreate(&ev0);
+            cudaEventCreate(&ev1);
+            cudaEventRecord(ev0, h->stream);
         }
-        CUDA_TRY(h, cudaEventRecord(ev_done, h->stream));
-        CUDA_TRY(h, cudaStreamWaitEvent(h->io_out, ev_done, 0));
-        for (int s = s0; s < s1; s++)
-            if ((e = copy_species_async(h, result(s).p, q_out[s], false, h->io_out))) return e;
+        auto result = [&](int s) -> DevBuf & { return mp ? h->qn[s] : (h->opts.rk3 ? h->q1s[s] : h->qn[s]); };
+        for (int gi = 0; gi < ngroups; gi++) {
+            const int s0 = S * gi / ngroups, s1 = S * (gi + 1) / ngroups;
+            cudaEvent_t ev_in = h->io_events[gi], ev_done = h->io_events[IO_GROUPS + gi];
+            for (int s = s0; s < s1; s++)
+                if ((e = copy_species_async(h, h->q[s].p, const_cast<float *>(q_in[s]), true, h->io_in))) return e;
+            CUDA_TRY(h, cudaEventRecord(ev_in, h->io_in));
+            CUDA_TRY(h, cudaStreamWaitEvent(h->stream, ev_in, 0));
+            if ((e = forcing_range(h, dt_seconds, s0, s1))) return e;
+            if ((e = mp ? mpdata_group(h, s0, s1) : std_group(h, s0, s1))) return e;
+            if (enforce_limits) {
+                for (int s = s0; s < s1; s++)
+                    icar::k_enforce_limits<<<blocks_for(h->n_cell, 256), 256, 0, h->stream>>>(h->g, result(s).p);
+                if ((e = check_launch(h, "enforce_limits", s1 - s0))) return e;
+            }
+            CUDA_TRY(h, cudaEventRecord(ev_done, h->stream));
+            CUDA_TRY(h, cudaStreamWaitEvent(h->io_out, ev_done, 0));
+            for (int s = s0; s < s1; s++)
+                if ((e = copy_species_async(h, result(s).p, q_out[s], false, h->io_out))) return e;
+        }
+        if (h->profiling) {
+            cudaEventRecord(ev1, h->stream);
+            h->events.emplace_back(ev0, ev1);
+            h->timed_launches += h->launches - before;
+        }
+        CUDA_TRY(h, cudaStreamSynchronize(h->io_out));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        for (int s = 0; s < S; s++) std::swap(h->q[s], result(s));
+        return ICAR_ADV_OK;
+    };
+    if ((e = pipeline())) {
+        cudaStreamSynchronize(h->io_in);
+        cudaStreamSynchronize(h->io_out);
+        cudaStreamSynchronize(h->stream);
+        return e;
     }
-    if (h->profiling) {
-        cudaEventRecord(ev1, h->stream);
-        h->events.emplace_back(ev0, ev1);
-        h->timed_launches += h->launches - before;
-    }
-    CUDA_TRY(h, cudaStreamSynchronize(h->io_out));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    for (int s = 0; s < S; s++) std::swap(h->q[s], result(s));
     return icar_adv_sync(h);
 }
 
@@ -2039,11 +2051,8 @@ extern "C" int icar_adv_advect_noalloc(const icar_adv_noalloc_args *a)
     if (!a->u || !a->v || !a->w || !a->density || !a->jacobian || !a->jacobian_u || !a->jacobian_v ||
         !a->jacobian_w || !a->advection_dz)
         return fail(nullptr, ICAR_ADV_BAD_ARG, "a wind or metric field pointer is NULL");
-    for (int s = 0; s < a->n_species; s++) {
+    for (int s = 0; s < a->n_species; s++)
         if (!a->q_in[s] || !a->q_out[s]) return fail(nullptr, ICAR_ADV_BAD_ARG, "species %d pointer is NULL", s);
-        if (a->q_in[s] == a->q_out[s])
-            return fail(nullptr, ICAR_ADV_BAD_ARG, "species %d: q_out must not alias q_in", s);
-    }
     Geo g;
     g.nx = a->nx;
     g.ny = a->ny;
@@ -2057,6 +2066,37 @@ extern "C" int icar_adv_advect_noalloc(const icar_adv_noalloc_args *a)
                     "domain %dx%dx%d needs %zu floats of scratch; the static scratch holds %zu "
                     "(use the handle API, which allocates, for larger domains)",
                     a->nx, a->ny, a->nz, need, NOALLOC_SCRATCH_FLOATS);
+    // The kernels stage whole rows with 16-byte asynchronous copies, so every
+    // array must start on a 16-byte boundary (the pitched rows then do too).
+    const void *inputs[9] = {a->u, a->v, a->w, a->density, a->jacobian, a->jacobian_u, a->jacobian_v,
+                             a->jacobian_w, a->advection_dz};
+    const char *input_names[9] = {"u", "v", "w", "density", "jacobian", "jacobian_u", "jacobian_v", "jacobian_w",
+                                  "advection_dz"};
+    for (int f = 0; f < 9; f++)
+        if ((uintptr_t)inputs[f] & 15u)
+            return fail(nullptr, ICAR_ADV_BAD_ARG, "%s is not 16-byte aligned", input_names[f]);
+    for (int s = 0; s < a->n_species; s++)
+        if (((uintptr_t)a->q_in[s] | (uintptr_t)a->q_out[s]) & 15u)
+            return fail(nullptr, ICAR_ADV_BAD_ARG, "species %d: q_in and q_out must be 16-byte aligned", s);
+    // Species run one after another on one stream, so an output that
+    // overlaps any input (or another output) would silently feed updated
+    // values into a later species: refuse every overlap.
+    auto overlaps = [](const void *p, size_t np, const void *q, size_t nq) {
+        const uintptr_t a0 = (uintptr_t)p, b0 = (uintptr_t)q;
+        return a0 < b0 + nq * sizeof(float) && b0 < a0 + np * sizeof(float);
+    };
+    const size_t n_in[9] = {nc, nv, nc, nc, nc, nc, nv, nc, nc};
+    for (int s = 0; s < a->n_species; s++) {
+        for (int t = 0; t < a->n_species; t++) {
+            if (overlaps(a->q_out[s], nc, a->q_in[t], nc))
+                return fail(nullptr, ICAR_ADV_BAD_ARG, "q_out[%d] overlaps q_in[%d] (no aliasing)", s, t);
+            if (t != s && overlaps(a->q_out[s], nc, a->q_out[t], nc))
+                return fail(nullptr, ICAR_ADV_BAD_ARG, "q_out[%d] overlaps q_out[%d] (no aliasing)", s, t);
+        }
+        for (int f = 0; f < 9; f++)
+            if (overlaps(a->q_out[s], nc, inputs[f], n_in[f]))
+                return fail(nullptr, ICAR_ADV_BAD_ARG, "q_out[%d] overlaps %s (no aliasing)", s, input_names[f]);
+    }
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
@@ -2075,13 +2115,16 @@ extern "C" int icar_adv_advect_noalloc(const icar_adv_noalloc_args *a)
     icar::k_mp_prep<<<blocks_for(nf, 256), 256, 0, st>>>(g, a->dx, a->dt, a->advect_density, a->u, a->v, a->w,
                                                        a->density, a->jacobian, a->jacobian_u, a->jacobian_v,
                                                        a->jacobian_w, a->advection_dz, Um, Vm, Wm, Gc, DJR, Wp);
-    const size_t ncell = (size_t)g.nx * g.nz * g.ny;
+    // the column-march donor-cell pass of the handle path, one species at a
+    // time through the one pass-1 field of the scratch
+    const dim3 gu((unsigned)((g.nx + icar::upf::BX - 1) / icar::upf::BX),
+                  (unsigned)((g.ny + icar::upf::BY - 1) / icar::upf::BY), 1u);
     for (int s = 0; s < a->n_species; s++) {
         icar::SpeciesPtrs sp{};
         sp.q0[0] = a->q_in[s];
         sp.q1[0] = q1;
         sp.out[0] = a->q_out[s];
-        icar::k_mp_upwind<<<blocks_for(ncell, 256), 256, 0, st>>>(g, sp, 1, 1, Um, Vm, Wm, Gc, DJR);
+        icar::k_mp_upwind_cols<<<gu, icar::upf::NT, icar::upf::SMEM, st>>>(g, sp, 1, 1, Um, Vm, Wm, Gc, DJR);
         icar::mp_corr_launch(st, 1, g, sp, 1, a->mpdata_fct ? 1 : 0, Um, Vm, Wp, Gc, DJR, a->advection_dz);
     }
     ce = cudaGetLastError();

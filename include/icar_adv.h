@@ -315,14 +315,18 @@ const char *icar_adv_batch_last_error(const icar_adv_batch_t *b);
  * round64 rounding up to a multiple of 64 (about 600 thousand cells, e.g.
  * 128x128x32); larger domains get ICAR_ADV_BAD_ARG with the sizes in the
  * message.  The scheme is advect() with MPDATA order 2 (FCT on or off):
- * every species is read from q_in[s] and the new state written to q_out[s]
- * (no aliasing); no boundary update.
+ * every species is read from q_in[s] and the new state written to q_out[s];
+ * no boundary update.  No output may overlap any input or another output
+ * (the species run one after another, so an overlap would feed updated
+ * values into a later species): such calls get ICAR_ADV_BAD_ARG.
  *
  * Device layout of every array: the reference's Fortran order with row pitch
  * P floats, element (i,k,j) at i + P*(k + nz*j); x-face fields (u,
  * jacobian_u) use i <= nx, y-face fields (v, jacobian_v) have ny+1 rows, cell
- * fields i < nx.  Padding columns are ignored on input and left untouched
- * on output.
+ * fields i < nx.  Every array must start on a 16-byte boundary (rows are
+ * staged with 16-byte copies); a misaligned pointer gets ICAR_ADV_BAD_ARG
+ * before anything is launched.  Padding columns are ignored on input and
+ * left untouched on output.
  *
  * The first call on a device sets that device up (it looks up the device
  * address of the static array and opts the kernel into its shared memory):
