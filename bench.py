@@ -54,6 +54,9 @@ def parse():
                    help="fused-kernel tile shape 0..3 (8/15/24/31 rows), or auto: chosen by hicar_b200.autotune")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
+    p.add_argument("--kernel", default="two-pass", choices=["two-pass", "single-pass", "single-pass-fast"],
+                   help="MPDATA kernels: the donor-cell kernel then the fused correction (two-pass), or the "
+                        "single-pass kernel with bit-exact or fast arithmetic")
     p.add_argument("--quick", action="store_true",
                    help="timed region only (no e2e, no CPU baseline): the profiling run")
     return p.parse_args()
@@ -229,6 +232,9 @@ def run_b200(args):
     if args.staged:
         d.use_staged_kernels(True)
     launch = set_launch_shape(d, args)
+    if not args.staged and args.kernel != "two-pass":
+        d.use_single_pass(fast=args.kernel == "single-pass-fast")
+        launch = {"kernel": args.kernel, "tile": "56 x 26 columns per CTA, 16 warps"}
     # a dedicated stream: the library and the timing events share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -333,7 +339,7 @@ def run_b200(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
-                       "kernel_path": "staged" if args.staged else "fused",
+                       "kernel_path": "staged" if args.staged else args.kernel,
                        "launch_shape": launch,
                        "l2": "inputs larger than L2 (12 fields x 42 MB per domain)",
                        "parallelism": f"replicas x{world}"},
@@ -353,7 +359,7 @@ def run_b200(args):
 def set_launch_shape(d, args) -> dict:
     """Tile shape and species group of the fused kernels for this domain."""
     from hicar_b200 import autotune
-    if args.tile_shape == "auto" and not args.staged:
+    if args.tile_shape == "auto" and not args.staged and args.kernel == "two-pass":
         c = autotune.tune_and_apply(d, fct=True)
         return {"tile_rows": c.rows, "species_group": c.species_group,
                 "chosen_by": "autotune: every shape and group timed on a synthetic domain of this grid shape"}

@@ -90,6 +90,7 @@ _PROTOS = {
     "icar_adv_enforce_limits": (C.c_int, [C.c_void_p]),
     "icar_adv_step": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "icar_adv_sync": (C.c_int, [C.c_void_p]),
+    "icar_adv_sync_timeout": (C.c_int, [C.c_void_p, C.c_double]),
     "icar_adv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "icar_adv_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "icar_adv_footprint": (C.c_int, [C.POINTER(Desc), C.POINTER(Opts), C.POINTER(C.c_int64)]),
@@ -118,6 +119,7 @@ _PROTOS = {
     "icar_adv_batch_set_species_group": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_step": (C.c_int, [C.c_void_p]),
     "icar_adv_batch_sync": (C.c_int, [C.c_void_p]),
+    "icar_adv_batch_sync_timeout": (C.c_int, [C.c_void_p, C.c_double]),
     "icar_adv_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "icar_adv_batch_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),

@@ -296,6 +296,15 @@ class Domain:
     def sync(self) -> None:
         L.check(L.load().icar_adv_sync(self.handle), self.handle)
 
+    def wait(self, timeout_s: float) -> bool:
+        """Bounded wait for the handle's queued work: True when it is done,
+        False when timeout_s passed first (the work stays queued)."""
+        code = L.load().icar_adv_sync_timeout(self.handle, C.c_double(timeout_s))
+        if code == L.TIMEOUT:
+            return False
+        L.check(code, self.handle)
+        return True
+
     def device_bytes(self) -> int:
         b = C.c_int64(0)
         L.check(L.load().icar_adv_device_bytes(self.handle, C.byref(b)), self.handle)
@@ -313,6 +322,15 @@ class Domain:
 
     def use_staged_kernels(self, staged: bool = True) -> None:
         L.check(L.load().icar_adv_set_path(self.handle, 1 if staged else 0), self.handle)
+
+    def use_single_pass(self, fast: bool = False) -> None:
+        """MPDATA order 2 through the single-pass kernel (donor-cell pass,
+        pseudo-velocities, limiter and corrective pass in one launch): bit-exact
+        arithmetic, or fast=True for the fast-arithmetic variant."""
+        L.check(L.load().icar_adv_set_path(self.handle, 3 if fast else 2), self.handle)
+
+    def set_path(self, path: int) -> None:
+        L.check(L.load().icar_adv_set_path(self.handle, int(path)), self.handle)
 
     def close(self) -> None:
         if self._h is not None:

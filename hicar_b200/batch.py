@@ -63,6 +63,15 @@ class Batch:
     def sync(self) -> None:
         self._check(self._lib.icar_adv_batch_sync(self._b), self._b)
 
+    def wait(self, timeout_s: float) -> bool:
+        """Bounded wait for the queued steps: True when they are done, False
+        when timeout_s passed first (the steps stay queued)."""
+        code = self._lib.icar_adv_batch_sync_timeout(self._b, C.c_double(timeout_s))
+        if code == L.TIMEOUT:
+            return False
+        self._check(code, self._b)
+        return True
+
     def profile(self, enable: bool = True) -> None:
         self._check(self._lib.icar_adv_batch_profile(self._b, int(enable)), self._b)
 

@@ -6,14 +6,18 @@
 // enqueued on the handle's stream; failures are returned as status codes with
 // a message, never by aborting.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <mutex>
+#include <thread>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/icar_adv.h"
@@ -26,6 +30,7 @@
 #include "batch_kernels.cuh"
 #include "wind_kernels.cuh"
 #include "mp_kernels.cuh"
+#include "mpdata_onepass.cuh"
 
 using icar::Geo;
 
@@ -84,7 +89,18 @@ struct icar_adv_domain {
     bool std_ready = false;      // fused standard-scheme buffers and kernel attributes
     bool std_staged_ready = false;
     DevBuf fx, fy, fz, ufx, ufy, ufz, dq, sin_, sout, temp;  // STD scratch
-    int path = 0;      // 0 = fused kernels (MPDATA order 2, every standard-scheme setting), 1 = staged kernels
+    // 0 = fused kernels (MPDATA order 2, every standard-scheme setting), 1 = staged kernels,
+    // 2 = single-pass MPDATA kernel (exact), 3 = single-pass MPDATA kernel (fast arithmetic)
+    int path = 0;
+    // single-pass kernel: TMA descriptors by device address (host cache),
+    // two device tables of descriptors (the species buffers alternate between
+    // two allocations, so two tables cover every step), timeout flag
+    std::unordered_map<const float *, CUtensorMap> tmaps;
+    CUtensorMap *map_dev[2] = {nullptr, nullptr};
+    std::vector<const float *> map_tag[2];
+    int map_next = 0;
+    int *op_err = nullptr;
+    bool op_ready = false;
     int mp_shape = 1;  // tile shape of the fused correction kernel (icar::mp_shape_ty)
     int sp_group = 0;  // species per thread of the fused upwind pass (0 = all)
     // diagnostics: launch counter and optional event timing of the species kernels
@@ -626,12 +642,172 @@ int ensure_fused(icar_adv_t *h)
     return ICAR_ADV_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Single-pass MPDATA kernel (mpdata_onepass.cuh): per-step fields from
+// k_mp_prep, then one launch for every species.  It needs no pass-1
+// buffers; its inputs are read through TMA descriptors.
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Descriptor of one pitched 3-D field (rows = ny or ny+1) for 64 x 1 x 32
+// plane boxes; cached per device address.
+int plane_map(icar_adv_t *h, const float *base, int rows, const CUtensorMap **out)
+{
+    auto it = h->tmaps.find(base);
+    if (it != h->tmaps.end()) {
+        *out = &it->second;
+        return ICAR_ADV_OK;
+    }
+    auto enc = tma_encoder();
+    if (!enc) return fail(h, ICAR_ADV_CUDA_ERROR, "cuTensorMapEncodeTiled is not available from the driver");
+    const Geo &g = h->g;
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)g.P, (cuuint64_t)g.nz, (cuuint64_t)rows};
+    cuuint64_t strides[2] = {(cuuint64_t)g.P * sizeof(float), (cuuint64_t)g.P * g.nz * sizeof(float)};
+    cuuint32_t box[3] = {(cuuint32_t)icar::op::PW, 1u, (cuuint32_t)icar::op::PH};
+    cuuint32_t es[3] = {1u, 1u, 1u};
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(h, ICAR_ADV_CUDA_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    auto ins = h->tmaps.emplace(base, m);
+    *out = &ins.first->second;
+    return ICAR_ADV_OK;
+}
+
+// The device table of descriptors for the current buffers: every species
+// input in adv_vars order, then U_m, V_m, W_m/dz, J*rho.  Two tables are
+// kept, tagged with the device addresses they describe; a table is rebuilt
+// (encode + one copy on the handle's stream) only when neither matches.
+int onepass_maps(icar_adv_t *h, const CUtensorMap **out)
+{
+    const int S = h->desc.n_species;
+    std::vector<const float *> want;
+    want.reserve(S + 4);
+    for (int s = 0; s < S; s++) want.push_back(h->q[s].p);
+    want.push_back(h->Um.p);
+    want.push_back(h->Vm.p);
+    want.push_back(h->Wp.p);
+    want.push_back(h->Gc.p);
+    for (int t = 0; t < 2; t++)
+        if (h->map_dev[t] && h->map_tag[t] == want) {
+            *out = h->map_dev[t];
+            return ICAR_ADV_OK;
+        }
+    const int t = h->map_next;
+    h->map_next ^= 1;
+    if (!h->map_dev[t]) CUDA_TRY(h, cudaMalloc(&h->map_dev[t], (size_t)(S + 4) * sizeof(CUtensorMap)));
+    std::vector<CUtensorMap> host(S + 4);
+    int e;
+    const CUtensorMap *m;
+    for (int s = 0; s < S + 4; s++) {
+        const int rows = s == S + 1 ? h->g.ny + 1 : h->g.ny;  // V_m has ny+1 rows
+        if ((e = plane_map(h, want[s], rows, &m))) return e;
+        host[s] = *m;
+    }
+    // ordered on the stream after any kernel still reading the old table
+    CUDA_TRY(h, cudaMemcpyAsync(h->map_dev[t], host.data(), host.size() * sizeof(CUtensorMap),
+                                cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->map_tag[t] = want;
+    *out = h->map_dev[t];
+    return ICAR_ADV_OK;
+}
+
+template <bool EXACT>
+cudaError_t onepass_attr()
+{
+    cudaError_t e = cudaFuncSetAttribute(icar::k_mpdata_onepass<EXACT, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)icar::op::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(icar::k_mpdata_onepass<EXACT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)icar::op::SMEM);
+    return e;
+}
+
+int ensure_onepass(icar_adv_t *h)
+{
+    const int S = h->desc.n_species;
+    int e;
+    if (!h->op_ready) {
+        h->qn.resize(S);
+        if ((e = alloc(h, h->Gc, h->n_cell)) || (e = alloc(h, h->DJR, h->n_cell)) || (e = alloc(h, h->Wp, h->n_cell)))
+            return e;
+        for (int s = 0; s < S; s++)
+            if ((e = alloc(h, h->qn[s], h->n_cell))) return e;
+        if (!h->op_err) {
+            CUDA_TRY(h, cudaMalloc(&h->op_err, sizeof(int)));
+            CUDA_TRY(h, cudaMemsetAsync(h->op_err, 0, sizeof(int), h->stream));
+        }
+        cudaError_t ce = onepass_attr<true>();
+        if (ce == cudaSuccess) ce = onepass_attr<false>();
+        if (ce != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "cudaFuncSetAttribute: %s", cudaGetErrorString(ce));
+        h->op_ready = true;
+    }
+    return ICAR_ADV_OK;
+}
+
+int onepass_tiles_x(const Geo &g) { return (g.nx + icar::op::TX - 1) / icar::op::TX; }
+int onepass_tiles_y(const Geo &g) { return (g.ny + icar::op::TY - 1) / icar::op::TY; }
+
+// The corrective pass and the donor-cell pass for species [s0, s1) in one
+// launch; results in qn.
+int mpdata_onepass_group(icar_adv_t *h, int s0, int s1)
+{
+    const Geo &g = h->g;
+    const int S = s1 - s0;
+    if (S <= 0) return ICAR_ADV_OK;
+    icar::OnePassParams prm{};
+    int e;
+    const CUtensorMap *table = nullptr;
+    if ((e = onepass_maps(h, &table))) return e;
+    prm.q0maps = table + s0;
+    prm.fmaps = table + h->desc.n_species;
+    for (int s = 0; s < S; s++) prm.out[s] = h->qn[s0 + s].p;
+    prm.Wm = h->Wm.p;
+    prm.DJR = h->DJR.p;
+    prm.dz = h->dz.p;
+    prm.err = h->op_err;
+    prm.g = g;
+    prm.nspecies = S;
+    prm.tiles_x = onepass_tiles_x(g);
+    const unsigned grid = (unsigned)(onepass_tiles_x(g) * onepass_tiles_y(g) * S);
+    const bool exact = h->path != 3, fct = h->opts.mpdata_fct != 0;
+    cudaEvent_t c0 = nullptr, c1 = nullptr;
+    if (h->profiling) {
+        cudaEventCreate(&c0);
+        cudaEventCreate(&c1);
+        cudaEventRecord(c0, h->stream);
+    }
+    if (exact && fct) icar::k_mpdata_onepass<true, true><<<grid, icar::op::NT, icar::op::SMEM, h->stream>>>(prm);
+    else if (exact) icar::k_mpdata_onepass<true, false><<<grid, icar::op::NT, icar::op::SMEM, h->stream>>>(prm);
+    else if (fct) icar::k_mpdata_onepass<false, true><<<grid, icar::op::NT, icar::op::SMEM, h->stream>>>(prm);
+    else icar::k_mpdata_onepass<false, false><<<grid, icar::op::NT, icar::op::SMEM, h->stream>>>(prm);
+    if (h->profiling) {
+        cudaEventRecord(c1, h->stream);
+        h->corr_events.emplace_back(c0, c1);
+    }
+    return check_launch(h, "single-pass MPDATA kernel", 1);
+}
+
 // Species-independent part of the fused MPDATA step (Courant fluxes, G,
 // DJR, W').
 int mpdata_prep(icar_adv_t *h, float dt)
 {
     const Geo &g = h->g;
-    int e = ensure_fused(h);
+    int e = h->path >= 2 ? ensure_onepass(h) : ensure_fused(h);
     if (e) return e;
     const size_t nf = (size_t)(g.nx + 1) * g.nz * (g.ny + 1);
     icar::k_mp_prep<<<blocks_for(nf, 256), 256, 0, h->stream>>>(
@@ -680,7 +856,7 @@ int mpdata_fused_step(icar_adv_t *h, float dt)
     const int S = h->desc.n_species;
     int e = mpdata_prep(h, dt);
     if (e) return e;
-    if ((e = mpdata_group(h, 0, S))) return e;
+    if ((e = h->path >= 2 ? mpdata_onepass_group(h, 0, S) : mpdata_group(h, 0, S))) return e;
     for (int s = 0; s < S; s++) std::swap(h->q[s], h->qn[s]);
     return ICAR_ADV_OK;
 }
@@ -786,7 +962,7 @@ int advect_impl(icar_adv_t *h, float dt)
     if (!(dt >= 0.0f) || !std::isfinite(dt)) return fail(h, ICAR_ADV_BAD_ARG, "dt must be finite and >= 0");
     const bool mp = h->opts.advection == ICAR_ADV_MPDATA;
     const bool fused_mp = mp && !h->opts.rk3 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct);
-    if (h->path == 0 && (fused_mp || !mp)) {
+    if ((h->path == 0 && (fused_mp || !mp)) || (h->path >= 2 && (fused_mp || !mp))) {
         cudaEvent_t ev0 = nullptr, ev1 = nullptr;
         int64_t before = h->launches;
         if (h->profiling) {
@@ -970,6 +1146,9 @@ int icar_adv_destroy(icar_adv_t *h)
         release(*b);
     if (h->acc_precip) cudaFree(h->acc_precip);
     if (h->mp_stop) cudaFree(h->mp_stop);
+    if (h->op_err) cudaFree(h->op_err);
+    for (auto *m : h->map_dev)
+        if (m) cudaFree(m);
     for (auto &b : h->q) release(b);
     for (auto &b : h->qn) release(b);
     for (auto &b : h->q1s) release(b);
@@ -1294,7 +1473,7 @@ int icar_adv_step_host(icar_adv_t *h, double dt_seconds, int32_t enforce_limits,
     const bool mp = h->opts.advection == ICAR_ADV_MPDATA;
     const bool fused_mp = mp && !h->opts.rk3 && icar::fused_eligible(h->opts.mpdata_order, h->opts.mpdata_fct);
     int e;
-    if (h->path != 0 || !(fused_mp || !mp) || h->opts.debug || S == 0) {
+    if (h->path == 1 || !(fused_mp || !mp) || h->opts.debug || S == 0) {
         // the unpipelined sequence (staged kernels, debug checks, RK3 MPDATA)
         for (int s = 0; s < S; s++)
             if ((e = copy_field(h, h->desc.species[s], const_cast<float *>(q_in[s]), nullptr, true))) return e;
@@ -1338,7 +1517,9 @@ int icar_adv_step_host(icar_adv_t *h, double dt_seconds, int32_t enforce_limits,
             CUDA_TRY(h, cudaEventRecord(ev_in, h->io_in));
             CUDA_TRY(h, cudaStreamWaitEvent(h->stream, ev_in, 0));
             if ((e = forcing_range(h, dt_seconds, s0, s1))) return e;
-            if ((e = mp ? mpdata_group(h, s0, s1) : std_group(h, s0, s1))) return e;
+            if ((e = mp ? (h->path >= 2 ? mpdata_onepass_group(h, s0, s1) : mpdata_group(h, s0, s1))
+                    : std_group(h, s0, s1)))
+            return e;
             if (enforce_limits) {
                 for (int s = s0; s < s1; s++)
                     icar::k_enforce_limits<<<blocks_for(h->n_cell, 256), 256, 0, h->stream>>>(h->g, result(s).p);
@@ -1378,11 +1559,60 @@ int icar_adv_step(icar_adv_t *h, double dt_seconds, int32_t enforce_limits)
     return ICAR_ADV_OK;
 }
 
+// After a sync: report (once) a tile whose TMA wait gave up in the
+// single-pass kernel.
+int check_op_err(icar_adv_t *h)
+{
+    if (!h->op_err) return ICAR_ADV_OK;
+    int flag = 0;
+    CUDA_TRY(h, cudaMemcpy(&flag, h->op_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!flag) return ICAR_ADV_OK;
+    CUDA_TRY(h, cudaMemset(h->op_err, 0, sizeof(int)));
+    if (flag == 2)
+        return fail(h, ICAR_ADV_CUDA_ERROR, "single-pass MPDATA kernel: a TMA operand was misaligned (loads skipped)");
+    return fail(h, ICAR_ADV_TIMEOUT, "a tile of the single-pass MPDATA kernel gave up waiting for its TMA loads");
+}
+
 int icar_adv_sync(icar_adv_t *h)
 {
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
     cudaSetDevice(h->desc.device);
     cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "stream sync: %s", cudaGetErrorString(e));
+    int r = check_op_err(h);
+    if (r) return r;
+    return check_mp_stop(h);
+}
+
+}  // extern "C"
+
+namespace {
+// Poll a stream until its work is done or `timeout_s` seconds have passed;
+// returns cudaSuccess, cudaErrorNotReady on timeout, or the stream's error.
+cudaError_t wait_stream(cudaStream_t st, double timeout_s)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned n = 0;; n++) {
+        cudaError_t e = cudaStreamQuery(st);
+        if (e != cudaErrorNotReady) return e;
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el >= timeout_s) return cudaErrorNotReady;
+        if (n > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int icar_adv_sync_timeout(icar_adv_t *h, double timeout_s)
+{
+    if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
+    if (!(timeout_s >= 0.0)) return fail(h, ICAR_ADV_BAD_ARG, "timeout must be >= 0 seconds");
+    cudaSetDevice(h->desc.device);
+    cudaError_t e = wait_stream(h->stream, timeout_s);
+    if (e == cudaErrorNotReady)
+        return fail(h, ICAR_ADV_TIMEOUT, "the handle's work did not finish within %.3f s (it is still queued)",
+                    timeout_s);
     if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "stream sync: %s", cudaGetErrorString(e));
     return check_mp_stop(h);
 }
@@ -1489,7 +1719,7 @@ int icar_adv_tile_shapes(int32_t *n_shapes, int32_t *rows)
 // kernels instead of the fused one (0 = fused when eligible, 1 = staged).
 int icar_adv_set_path(icar_adv_t *h, int32_t path)
 {
-    if (!h || path < 0 || path > 1) return fail(h, ICAR_ADV_BAD_ARG, "bad path");
+    if (!h || path < 0 || path > 3) return fail(h, ICAR_ADV_BAD_ARG, "bad path");
     h->path = path;
     return ICAR_ADV_OK;
 }
@@ -1911,6 +2141,18 @@ int icar_adv_batch_sync(icar_adv_batch_t *b)
     if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
     cudaSetDevice(b->device);
     BCUDA(b, cudaStreamSynchronize(b->stream));
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_sync_timeout(icar_adv_batch_t *b, double timeout_s)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    if (!(timeout_s >= 0.0)) return bfail(b, ICAR_ADV_BAD_ARG, "timeout must be >= 0 seconds");
+    cudaSetDevice(b->device);
+    cudaError_t e = wait_stream(b->stream, timeout_s);
+    if (e == cudaErrorNotReady)
+        return bfail(b, ICAR_ADV_TIMEOUT, "the batch's steps did not finish within %.3f s (still queued)", timeout_s);
+    if (e != cudaSuccess) return bfail(b, ICAR_ADV_CUDA_ERROR, "stream sync: %s", cudaGetErrorString(e));
     return ICAR_ADV_OK;
 }
 

@@ -182,6 +182,21 @@ def smooth_field(shape, rng: np.random.Generator, coarse: int = 8) -> np.ndarray
     return g[oy:oy + ny, oz:oz + nz, ox:ox + nx]
 
 
+def correlated_noise(shape, rng: np.random.Generator, L: int = 8, Lz: int = 4) -> np.ndarray:
+    """Smooth unit-variance noise: normal noise on a grid L cells apart (Lz
+    levels apart), interpolated trilinearly to the full grid.  Used for the
+    seeded wind perturbations: cell-to-cell (white) wind noise makes the flow
+    strongly convergent from one cell to the next, and the reference scheme
+    itself then grows without bound within tens of steps."""
+    from scipy.ndimage import zoom
+    ny, nz, nx = shape
+    c = rng.standard_normal((ny // L + 3, nz // Lz + 3, nx // L + 3))
+    f = zoom(c, (L, Lz, L), order=1)
+    oy, oz, ox = (int(rng.integers(0, L)), int(rng.integers(0, Lz)), int(rng.integers(0, L)))
+    f = f[oy:oy + ny, oz:oz + nz, ox:ox + nx]
+    return ((f - f.mean()) / (f.std() + 1e-30)).astype(F32)
+
+
 def hydrometeor(shape, rng, zero_frac=0.7, median=1e-4, sigma=1.0) -> np.ndarray:
     """Lognormal mixing ratio with an exact-zero fraction, zeros clustered."""
     s = smooth_field(shape, rng)
@@ -226,8 +241,8 @@ def build_case(nx, ny, nz, dx, dz_levels, terrain, U, V=0.0, mountain_N=None, wi
         u[:, :, 1:nx] += (up[:, :, 1:] + up[:, :, :-1]) / 2
         v[1:ny] += (vp[1:] + vp[:-1]) / 2
     if wind_noise > 0:
-        u += (wind_noise * abs(U) * rng.standard_normal(u.shape)).astype(F32)
-        v += (wind_noise * abs(U) * rng.standard_normal(v.shape)).astype(F32)
+        u += (wind_noise * abs(U) * correlated_noise(u.shape, rng)).astype(F32)
+        v += (wind_noise * abs(U) * correlated_noise(v.shape, rng)).astype(F32)
     w = calc_w(u, v, ju, jv, jw, adz, dx)
     density = (1.225 * np.exp(-z / 8500.0)).astype(F32)
     sp = make_species(species, z, rng, qv_noise=qv_noise)
@@ -364,8 +379,17 @@ def device_member(nx: int, ny: int, nz: int, seed: int, device: int = 0, dx: flo
     jw[:, :nz - 1] = (dzi[:, :-1] * jac[:, :-1] + dzi[:, 1:] * jac[:, 1:]) / (dzi[:, :-1] + dzi[:, 1:])
     adz = torch.full((ny, nz, nx), dz, device=dev, dtype=f32)
     U = float(8.0 + 4.0 * r(1).item()) if U is None else float(U)
-    u = U + noise * U * n(ny, nz, nx + 1)
-    v = noise * U * n(ny + 1, nz, nx)
+
+    def smooth(*shape, L=8, Lz=4):
+        # unit-variance noise interpolated trilinearly from a grid L cells apart
+        sy, sz, sx = shape
+        c = n(1, 1, sy // L + 3, sz // Lz + 3, sx // L + 3)
+        f = torch.nn.functional.interpolate(c, scale_factor=(L, Lz, L), mode="trilinear", align_corners=False)
+        f = f[0, 0, :sy, :sz, :sx]
+        return (f - f.mean()) / (f.std() + 1e-30)
+
+    u = U + noise * U * smooth(ny, nz, nx + 1)
+    v = noise * U * smooth(ny + 1, nz, nx)
     div = ((u * ju)[:, :, 1:] - (u * ju)[:, :, :-1] + (v * jv)[1:] - (v * jv)[:-1]) / dx
     w = torch.empty(ny, nz, nx, device=dev, dtype=f32)
     w[:, 0] = (0 - div[:, 0] * adz[:, 0]) / jw[:, 0]

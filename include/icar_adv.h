@@ -243,6 +243,12 @@ int icar_adv_set_precipitation(icar_adv_t *h, const double *rain, const double *
 /* Block until the handle's stream has drained; reports device-side errors. */
 int icar_adv_sync(icar_adv_t *h);
 
+/* Bounded wait (no reference counterpart; the reference's calls are
+ * synchronous): like icar_adv_sync, but gives up after timeout_s seconds
+ * and returns ICAR_ADV_TIMEOUT with the work still queued (a later sync
+ * can wait for it).  timeout_s = 0 asks whether the work is done. */
+int icar_adv_sync_timeout(icar_adv_t *h, double timeout_s);
+
 /* Use an external CUDA stream (cudaStream_t passed as void*; NULL = the
  * handle's own stream). */
 int icar_adv_set_stream(icar_adv_t *h, void *cuda_stream);
@@ -291,6 +297,8 @@ int icar_adv_batch_set_tile_shape(icar_adv_batch_t *b, int32_t shape);
 int icar_adv_batch_set_species_group(icar_adv_batch_t *b, int32_t group);
 int icar_adv_batch_step(icar_adv_batch_t *b);
 int icar_adv_batch_sync(icar_adv_batch_t *b);
+/* Bounded wait for the batch's steps; ICAR_ADV_TIMEOUT after timeout_s. */
+int icar_adv_batch_sync_timeout(icar_adv_batch_t *b, double timeout_s);
 int icar_adv_batch_set_stream(icar_adv_batch_t *b, void *cuda_stream);
 /* Event timing of every step launched while enabled; reading synchronises. */
 int icar_adv_batch_profile(icar_adv_batch_t *b, int32_t enable);

@@ -1,0 +1,97 @@
+"""Parity at the stated configurations and step counts (GPU).
+
+Config 2 at full size (512x512x40, 12 FP32 fields, dt 4 s) over 100 steps,
+and a config-3 ensemble draw at full member sizes (nx, ny ~ U[64, 384], nz ~
+U[20, 50], 12 fields) advanced 20 steps in one batch.  The bit-exact kernels
+must equal the FP32 oracle cell for cell; the error against the FP64 oracle
+(the same scheme in double precision) is printed for every field.  The path's
+tolerance (max relative error <= 1e-4 after 100 steps, floor
+1e-6 * max|q|) is asserted against the FP32 oracle.
+
+The oracle runs take a few minutes on the host cores; their results are
+computed once per module and shared.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from hicar_b200 import synth
+from hicar_b200.advection import Domain, Options, adv_init, advect, step
+from hicar_b200.batch import Batch
+
+pytestmark = pytest.mark.gpu
+
+FLOOR = 1e-6
+
+
+def rel_err(a, ref):
+    """max |a-ref| / max(|ref|, 1e-6 * max|ref|)."""
+    ref = ref.astype(np.float64)
+    scale = max(float(np.abs(ref).max()), 1e-30)
+    den = np.maximum(np.abs(ref), FLOOR * scale)
+    return float((np.abs(a.astype(np.float64) - ref) / den).max())
+
+
+@pytest.fixture(scope="module")
+def config2_100(oracle_lib):
+    O = oracle_lib
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    case = synth.config2(seed=2)
+    ref32 = O.run_steps(case, O.make_opts(), case.dt, 100)
+    ref64 = O.run_steps(case, O.make_opts(), case.dt, 100, dtype=np.float64)
+    return case, ref32, ref64
+
+
+def test_config2_full_size_100_steps(config2_100):
+    case, ref32, ref64 = config2_100
+    opts = Options()
+    d = Domain.from_case(case)
+    adv_init(d, opts)
+    for _ in range(100):
+        advect(d, opts, case.dt)
+    out = {k: d.fetch(k).copy() for k in case.species}
+    d.close()
+    lines = []
+    for k in case.species:
+        e32 = rel_err(out[k], ref32[k])
+        assert e32 <= 1e-4, f"{k}: rel err {e32:.3e} vs the FP32 oracle after 100 steps"
+        nd = int((out[k] != ref32[k]).sum())
+        assert nd == 0, f"{k}: {nd} cells differ from the FP32 oracle after 100 steps"
+        lines.append(f"{k} {rel_err(out[k], ref64[k]):.2e}")
+    print("config 2, 512x512x40, 100 steps: bit-exact vs FP32 oracle; error vs FP64 oracle: " + ", ".join(lines))
+
+
+def test_config3_ensemble_full_member_sizes_20_steps(oracle_lib):
+    """The first eight members of the config-3 draw the benchmark uses
+    (ensemble_shapes(64, 7)), at their full sizes and with all 12 fields,
+    advanced together in one batch for 20 steps; every member equals the
+    FP32 oracle cell for cell."""
+    O = oracle_lib
+    shapes = synth.ensemble_shapes(64, 7)[:8]
+    cases = [synth.ensemble_member(7 * 1000 + i, nx, ny, nz) for i, (nx, ny, nz) in enumerate(shapes)]
+    b = Batch()
+    doms = []
+    for c in cases:
+        d = Domain.from_case(c)
+        adv_init(d, Options())
+        b.add(d, c.dt)
+        doms.append(d)
+    nsteps = 20
+    for _ in range(nsteps):
+        b.step()
+    b.sync()
+    report = []
+    for c, d in zip(cases, doms):
+        ref = O.run_steps(c, O.make_opts(), c.dt, nsteps)
+        ref64 = O.run_steps(c, O.make_opts(), c.dt, nsteps, dtype=np.float64)
+        worst = 0.0
+        for k in c.species:
+            got = d.fetch(k)
+            assert np.array_equal(got, ref[k]), (c.nx, c.ny, c.nz, k)
+            worst = max(worst, rel_err(got, ref64[k]))
+        report.append(f"{c.nx}x{c.ny}x{c.nz}: {worst:.2e}")
+    b.close()
+    for d in doms:
+        d.close()
+    print("config 3 members, 20 steps, bit-exact vs FP32 oracle; worst field error vs FP64: " + "; ".join(report))

@@ -84,3 +84,32 @@ def test_step_host_rejects_bad_arguments():
     with pytest.raises(ValueError):
         step_host(d, Options(), 1.0, {"qv": np.zeros((3, 3, 3), np.float32)})
     d.close()
+
+
+def test_bounded_wait_reports_timeout_then_completes(oracle_lib):
+    """icar_adv_sync_timeout: with 30 steps of a 256x256x40 x 12-field
+    domain queued (tens of milliseconds of device work), a zero timeout
+    returns ICAR_ADV_TIMEOUT and leaves the work queued; a generous one then
+    returns OK, and the result equals the same steps waited for with
+    icar_adv_sync.  Nothing on the device is made to hang: the work simply
+    has not finished when the first wait gives up."""
+    from hicar_b200 import synth
+    from hicar_b200.advection import Domain, Options, adv_init, advect
+    case = synth.config2(seed=12, nx=256, ny=256, nz=40)
+    opts = Options()
+    outs = []
+    for bounded in (True, False):
+        d = Domain.from_case(case)
+        adv_init(d, opts)
+        d.sync()
+        for _ in range(30):
+            advect(d, opts, case.dt)
+        if bounded:
+            assert d.wait(0.0) is False
+            assert d.wait(120.0) is True
+        else:
+            d.sync()
+        outs.append({k: d.fetch(k).copy() for k in ("qv", "theta")})
+        d.close()
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k])
