@@ -34,6 +34,8 @@ sys.path.insert(0, str(ROOT))
 import numpy as np  # noqa: E402
 
 METRIC = "MPDATA cell-species updates/s"
+# --kernel -> icar_adv_set_path / icar_adv_batch_set_path
+KERNEL_PATH = {"two-pass": 0, "single-pass": 2, "single-pass-fast": 3}
 UNIT = "cell-species updates/s"
 
 
@@ -729,6 +731,7 @@ def run_ensemble(args):
             d.set_forcing(k, q, None)           # fixed inflow boundaries
         adv_init(d, opts)
         L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
+        d.set_path(KERNEL_PATH[args.kernel])
         doms.append(d)
     cs_step = sum(c.cells() * len(c.species) for c in cases)
 
@@ -761,9 +764,13 @@ def run_ensemble(args):
     # ---- batched: every member in one graph launch per step
     b = Batch(device=local)
     b.set_stream(stream.cuda_stream)
+    b.set_path(KERNEL_PATH[args.kernel])
     for d, c in zip(doms, cases):
         b.add(d, c.dt)
-    if args.tile_shape == "auto":
+    shape = 1
+    if args.kernel != "two-pass":
+        pass                                    # the single-pass kernel has one tile shape
+    elif args.tile_shape == "auto":
         from hicar_b200 import autotune
         shape = autotune.tune_batch(b)
     else:
@@ -835,8 +842,10 @@ def run_ensemble(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": ENSEMBLE_DESC, "members": len(cases), "cell_species_per_step": cs_step,
                        "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
-                       "tile_shape_rows": [8, 16, 24, 32][shape],
-                       "tile_shape_chosen_by": "autotune cost model" if args.tile_shape == "auto" else "--tile-shape",
+                       "kernel": args.kernel,
+                       "tile_shape_rows": [8, 16, 24, 32][shape] if args.kernel == "two-pass" else 26,
+                       "tile_shape_chosen_by": ("autotune cost model" if args.tile_shape == "auto" else "--tile-shape")
+                       if args.kernel == "two-pass" else "fixed 56 x 26 tiles",
                        "l2": "inputs larger than L2 (~6 GB of species per step)",
                        "parallelism": f"replicas x{world}"},
             "plain": {"value": plain_value, "steps": plain_steps, "ms_per_step": plain_ms / plain_steps,

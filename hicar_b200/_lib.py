@@ -120,6 +120,7 @@ _PROTOS = {
     "icar_adv_batch_step": (C.c_int, [C.c_void_p]),
     "icar_adv_batch_sync": (C.c_int, [C.c_void_p]),
     "icar_adv_batch_sync_timeout": (C.c_int, [C.c_void_p, C.c_double]),
+    "icar_adv_batch_set_path": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "icar_adv_batch_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "icar_adv_batch_profile_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),

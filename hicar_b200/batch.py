@@ -51,6 +51,11 @@ class Batch:
     def set_tile_shape(self, shape: int) -> None:
         self._check(self._lib.icar_adv_batch_set_tile_shape(self._b, int(shape)), self._b)
 
+    def set_path(self, path: int) -> None:
+        """0: donor-cell kernel + fused correction (default); 2: single-pass
+        kernel, bit-exact; 3: single-pass kernel, fast arithmetic."""
+        self._check(self._lib.icar_adv_batch_set_path(self._b, int(path)), self._b)
+
     def set_species_group(self, group: int) -> None:
         self._check(self._lib.icar_adv_batch_set_species_group(self._b, int(group)), self._b)
 

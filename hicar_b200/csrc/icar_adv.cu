@@ -1750,6 +1750,15 @@ struct icar_adv_batch {
     int4 *d_items = nullptr;
     size_t items_cap = 0;
     int n_prep = 0, n_up = 0, n_force = 0, n_pairs = 0, n_items = 0, ctas = 0;
+    // single-pass kernel (path 2 exact, 3 fast; 0 = the two-pass kernels):
+    // per-member kernel parameters for both buffer parities, their TMA
+    // descriptor tables, and one timeout flag for the whole batch
+    int path = 0;
+    icar::OnePassParams *d_opp[2] = {nullptr, nullptr};
+    size_t opp_cap = 0;
+    CUtensorMap *d_bmaps = nullptr;
+    size_t bmaps_cap = 0;
+    int *d_operr = nullptr;
     size_t off_up = 0, off_f = 0, off_counter = 0;
     cudaGraph_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -1835,7 +1844,7 @@ void fill_member(icar::BatchMember &m, icar_adv_t *h, double dt, int parity)
         float *nxt = parity == 0 ? h->qn[s].p : h->q[s].p;
         m.q0[s] = cur;
         m.out[s] = nxt;
-        m.q1[s] = h->q1s[s].p;
+        m.q1[s] = s < (int)h->q1s.size() ? h->q1s[s].p : nullptr;
         m.forcing[s] = h->forcing[s].p;
         m.dqdt[s] = h->dqdt[s].p;
     }
@@ -1852,8 +1861,42 @@ int build_tables(icar_adv_batch_t *b)
     std::vector<int2> pairs;
     std::vector<int4> items;
     const int ty = icar::mp_shape_ty(b->shape);
+    const bool onepass = b->path >= 2;
+    std::vector<icar::OnePassParams> opp[2];
+    std::vector<CUtensorMap> maps;
+    std::vector<size_t> map_base[2];
+    if (onepass) {
+        opp[0].resize(std::max(M, 1));
+        opp[1].resize(std::max(M, 1));
+        map_base[0].resize(M);
+        map_base[1].resize(M);
+        if (!b->d_operr) {
+            BCUDA(b, cudaMalloc(&b->d_operr, sizeof(int)));
+            BCUDA(b, cudaMemsetAsync(b->d_operr, 0, sizeof(int), b->stream));
+        }
+    }
     for (int m = 0; m < M; m++) {
         icar_adv_t *h = b->members[m];
+        if (onepass) {
+            int r = ensure_onepass(h);
+            if (r) return bfail(b, r, "member scratch: %s", h->err.c_str());
+            // descriptors of both parities: species inputs, then U_m, V_m, W_m/dz, J*rho
+            for (int pp = 0; pp < 2; pp++) {
+                map_base[pp][m] = maps.size();
+                const int S = h->desc.n_species;
+                for (int f = 0; f < S + 4; f++) {
+                    const float *base = f < S ? (pp == 0 ? h->q[f].p : h->qn[f].p)
+                                              : (f == S ? h->Um.p : f == S + 1 ? h->Vm.p : f == S + 2 ? h->Wp.p : h->Gc.p);
+                    const CUtensorMap *mp;
+                    if ((r = plane_map(h, base, f == S + 1 ? h->g.ny + 1 : h->g.ny, &mp)))
+                        return bfail(b, r, "%s", h->err.c_str());
+                    maps.push_back(*mp);
+                }
+            }
+        } else {
+            int r = ensure_fused(h);
+            if (r) return bfail(b, r, "member scratch: %s", h->err.c_str());
+        }
         // members' buffers hold "current" in q at the batch's parity 0
         fill_member(mem[0][m], h, b->dts[m], b->parity == 0 ? 0 : 1);
         fill_member(mem[1][m], h, b->dts[m], b->parity == 0 ? 1 : 0);
@@ -1867,11 +1910,56 @@ int build_tables(icar_adv_batch_t *b)
                 fpre.push_back(fpre.back() + (int)(((size_t)h->nzone * g.nz + 255) / 256));
             }
         }
-        const int tx = icar::mp_tiles_x(g), tyn = icar::mp_tiles_y(g, ty);
-        for (int s = 0; s < h->desc.n_species; s++)
-            for (int a = 0; a < tyn; a++)
-                for (int c = 0; c < tx; c++)
-                    items.push_back(make_int4(m, s, c * icar::mpf::TX - 2, 1 + a * ty));
+        if (onepass) {
+            const int tx = onepass_tiles_x(g), tyn = onepass_tiles_y(g);
+            for (int s = 0; s < h->desc.n_species; s++)
+                for (int a = 0; a < tyn; a++)
+                    for (int c = 0; c < tx; c++)
+                        items.push_back(make_int4(m, s, c * icar::op::TX, a * icar::op::TY));
+        } else {
+            const int tx = icar::mp_tiles_x(g), tyn = icar::mp_tiles_y(g, ty);
+            for (int s = 0; s < h->desc.n_species; s++)
+                for (int a = 0; a < tyn; a++)
+                    for (int c = 0; c < tx; c++)
+                        items.push_back(make_int4(m, s, c * icar::mpf::TX - 2, 1 + a * ty));
+        }
+    }
+    if (onepass && !maps.empty() && (maps.size() > b->bmaps_cap || !b->d_bmaps)) {
+        if (b->d_bmaps) cudaFree(b->d_bmaps);  // synchronises: queued launches may read it
+        b->d_bmaps = nullptr;
+        b->bmaps_cap = 0;
+        const size_t cap = maps.size() * 3 / 2 + 16;
+        BCUDA(b, cudaMalloc(&b->d_bmaps, cap * sizeof(CUtensorMap)));
+        b->bmaps_cap = cap;
+    }
+    if (onepass) {
+        for (int pp = 0; pp < 2; pp++)
+            for (int m = 0; m < M; m++) {
+                icar_adv_t *h = b->members[m];
+                icar::OnePassParams &q = opp[pp][m];
+                memset(&q, 0, sizeof(q));
+                const int S = h->desc.n_species;
+                q.q0maps = b->d_bmaps + map_base[pp][m];
+                q.fmaps = q.q0maps + S;
+                for (int s2 = 0; s2 < S; s2++) q.out[s2] = pp == 0 ? h->qn[s2].p : h->q[s2].p;
+                q.Wm = h->Wm.p;
+                q.DJR = h->DJR.p;
+                q.dz = h->dz.p;
+                q.err = b->d_operr;
+                q.g = h->g;
+                q.nspecies = S;
+                q.tiles_x = onepass_tiles_x(h->g);
+            }
+        if ((size_t)std::max(M, 1) > b->opp_cap || !b->d_opp[0]) {
+            for (int pp = 0; pp < 2; pp++) {
+                if (b->d_opp[pp]) cudaFree(b->d_opp[pp]);
+                b->d_opp[pp] = nullptr;
+            }
+            b->opp_cap = 0;
+            const size_t cap = std::max<size_t>(M, 16);
+            for (int pp = 0; pp < 2; pp++) BCUDA(b, cudaMalloc(&b->d_opp[pp], cap * sizeof(icar::OnePassParams)));
+            b->opp_cap = cap;
+        }
     }
     // longest columns first (cost ~ nz per tile), so the tail of the
     // persistent launch is made of short items
@@ -1909,10 +1997,11 @@ int build_tables(icar_adv_batch_t *b)
     // staging sets alternate; a set is reused only after its previous upload
     // has been consumed.
     const size_t bm = sizeof(icar::BatchMember) * std::max(M, 1);
-    const size_t seg[5] = {bm, bm, sizeof(int) * ints.size(), sizeof(int2) * pairs.size(),
-                           sizeof(int4) * items.size()};
-    size_t off[5], total = 0;
-    for (int i = 0; i < 5; i++) {
+    const size_t po = onepass ? sizeof(icar::OnePassParams) * std::max(M, 1) : 0;
+    const size_t seg[8] = {bm, bm, sizeof(int) * ints.size(), sizeof(int2) * pairs.size(),
+                           sizeof(int4) * items.size(), po, po, sizeof(CUtensorMap) * maps.size()};
+    size_t off[8], total = 0;
+    for (int i = 0; i < 8; i++) {
         off[i] = total;
         total += (seg[i] + 255) / 256 * 256;
     }
@@ -1932,14 +2021,21 @@ int build_tables(icar_adv_batch_t *b)
     memcpy(st + off[2], ints.data(), seg[2]);
     if (seg[3]) memcpy(st + off[3], pairs.data(), seg[3]);
     if (seg[4]) memcpy(st + off[4], items.data(), seg[4]);
+    if (seg[5]) memcpy(st + off[5], opp[0].data(), seg[5]);
+    if (seg[6]) memcpy(st + off[6], opp[1].data(), seg[6]);
+    if (seg[7]) memcpy(st + off[7], maps.data(), seg[7]);
     BCUDA(b, cudaMemcpyAsync(b->d_mem[0], st + off[0], seg[0], cudaMemcpyHostToDevice, b->stream));
     BCUDA(b, cudaMemcpyAsync(b->d_mem[1], st + off[1], seg[1], cudaMemcpyHostToDevice, b->stream));
     BCUDA(b, cudaMemcpyAsync(b->d_ints, st + off[2], seg[2], cudaMemcpyHostToDevice, b->stream));
     if (seg[3]) BCUDA(b, cudaMemcpyAsync(b->d_pairs, st + off[3], seg[3], cudaMemcpyHostToDevice, b->stream));
     if (seg[4]) BCUDA(b, cudaMemcpyAsync(b->d_items, st + off[4], seg[4], cudaMemcpyHostToDevice, b->stream));
+    if (seg[5]) BCUDA(b, cudaMemcpyAsync(b->d_opp[0], st + off[5], seg[5], cudaMemcpyHostToDevice, b->stream));
+    if (seg[6]) BCUDA(b, cudaMemcpyAsync(b->d_opp[1], st + off[6], seg[6], cudaMemcpyHostToDevice, b->stream));
+    if (seg[7]) BCUDA(b, cudaMemcpyAsync(b->d_bmaps, st + off[7], seg[7], cudaMemcpyHostToDevice, b->stream));
     BCUDA(b, cudaEventRecord(b->stage_done[t], b->stream));
     b->stage_turn ^= 1;
-    b->ctas = std::min(std::max(b->n_items, 1), icar::batch_corr_max_ctas(b->shape, b->fct, b->nsm));
+    b->ctas = onepass ? std::min(std::max(b->n_items, 1), b->nsm)  // one 192 KB CTA per SM
+                      : std::min(std::max(b->n_items, 1), icar::batch_corr_max_ctas(b->shape, b->fct, b->nsm));
     b->tables_dirty = false;
     return ICAR_ADV_OK;
 }
@@ -1952,6 +2048,20 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
     if (b->n_force > 0)
         icar::k_batch_forcing<<<b->n_force, 256, 0, st>>>(mem, b->d_ints + b->off_f, b->d_pairs, b->n_pairs);
     if (b->n_prep > 0) icar::k_batch_prep<<<b->n_prep, 256, 0, st>>>(mem, b->d_ints, M);
+    if (b->path >= 2) {
+        cudaMemsetAsync(b->d_ints + b->off_counter, 0, sizeof(int), st);
+        if (b->n_items > 0) {
+            const icar::OnePassParams *opp = b->d_opp[p];
+            int *ctr = b->d_ints + b->off_counter;
+            const int n = b->n_items, c = b->ctas;
+            const size_t sm = icar::op::SMEM;
+            if (b->path == 2 && b->fct) icar::k_batch_onepass<true, true><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
+            else if (b->path == 2) icar::k_batch_onepass<true, false><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
+            else if (b->fct) icar::k_batch_onepass<false, true><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
+            else icar::k_batch_onepass<false, false><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
+        }
+        return;
+    }
     if (b->n_up > 0)
         icar::k_batch_upwind<<<b->n_up, icar::upf::NT, icar::upf::SMEM, st>>>(mem, b->d_ints + b->off_up, M,
                                                                            b->sp_group);
@@ -1959,6 +2069,19 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
     if (b->n_items > 0)
         icar::batch_corr_launch(st, b->shape, b->ctas, b->fct, mem, b->d_items, b->n_items,
                                 b->d_ints + b->off_counter);
+}
+
+cudaError_t batch_onepass_setup()
+{
+    const int sm = (int)icar::op::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(icar::k_batch_onepass<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(icar::k_batch_onepass<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(icar::k_batch_onepass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(icar::k_batch_onepass<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return e;
 }
 
 int build_graphs(icar_adv_batch_t *b)
@@ -1993,6 +2116,7 @@ int icar_adv_batch_create(int32_t device, icar_adv_batch_t **out)
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = icar::mp_corr_setup();
     if (e == cudaSuccess) e = icar::batch_setup();
+    if (e == cudaSuccess) e = batch_onepass_setup();
     if (e != cudaSuccess) {
         int code = bfail(nullptr, ICAR_ADV_CUDA_ERROR, "batch setup failed: %s", cudaGetErrorString(e));
         if (b->stream) cudaStreamDestroy(b->stream);
@@ -2017,7 +2141,7 @@ int icar_adv_batch_add(icar_adv_batch_t *b, icar_adv_t *h, double dt_seconds)
     cudaSetDevice(b->device);
     int e = ensure_ready(h);
     if (e) return bfail(b, e, "member not ready: %s", h->err.c_str());
-    e = ensure_fused(h);
+    e = b->path >= 2 ? ensure_onepass(h) : ensure_fused(h);
     if (e) return bfail(b, e, "member scratch: %s", h->err.c_str());
     // order the member's pending work before the batch's, then share the stream
     cudaStreamSynchronize(h->stream);
@@ -2141,6 +2265,27 @@ int icar_adv_batch_sync(icar_adv_batch_t *b)
     if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
     cudaSetDevice(b->device);
     BCUDA(b, cudaStreamSynchronize(b->stream));
+    if (b->d_operr) {
+        int flag = 0;
+        BCUDA(b, cudaMemcpy(&flag, b->d_operr, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flag) {
+            BCUDA(b, cudaMemset(b->d_operr, 0, sizeof(int)));
+            return bfail(b, flag == 2 ? ICAR_ADV_CUDA_ERROR : ICAR_ADV_TIMEOUT,
+                         flag == 2 ? "single-pass MPDATA kernel: a TMA operand was misaligned (loads skipped)"
+                                   : "a tile of the single-pass MPDATA kernel gave up waiting for its TMA loads");
+        }
+    }
+    return ICAR_ADV_OK;
+}
+
+int icar_adv_batch_set_path(icar_adv_batch_t *b, int32_t path)
+{
+    if (!b) return bfail(nullptr, ICAR_ADV_BAD_ARG, "batch is NULL");
+    if (path != 0 && path != 2 && path != 3) return bfail(b, ICAR_ADV_BAD_ARG, "batch path must be 0, 2 or 3");
+    if (path != b->path) {
+        b->path = path;
+        b->tables_dirty = b->graph_dirty = true;
+    }
     return ICAR_ADV_OK;
 }
 
@@ -2224,6 +2369,10 @@ int icar_adv_batch_destroy(icar_adv_batch_t *b)
     if (b->d_ints) cudaFree(b->d_ints);
     if (b->d_pairs) cudaFree(b->d_pairs);
     if (b->d_items) cudaFree(b->d_items);
+    for (auto *q : b->d_opp)
+        if (q) cudaFree(q);
+    if (b->d_bmaps) cudaFree(b->d_bmaps);
+    if (b->d_operr) cudaFree(b->d_operr);
     for (int t = 0; t < 2; t++) {
         if (b->stage[t]) cudaFreeHost(b->stage[t]);
         if (b->stage_done[t]) cudaEventDestroy(b->stage_done[t]);

@@ -63,7 +63,7 @@ constexpr int S_V2 = 21;             // unlimited v2 of the current level
 constexpr int S_BYI = 22, S_BYO = 23;  // y-limiter betas of the current level
 constexpr int NPLANES = 24;
 constexpr size_t SMEM = (size_t)NPLANES * PLANE * sizeof(float) + 128;
-constexpr uint32_t WAIT_LIMIT = 1u << 22;  // mbarrier polls before a wait gives up
+constexpr uint64_t WAIT_NS = 2000000000ull;  // a TMA wait gives up after 2 s
 constexpr int MAXS = 32;             // species per launch
 }  // namespace op
 
@@ -163,11 +163,17 @@ __device__ __forceinline__ float beta(float num, float den)
 }
 
 // Limited pseudo-velocity at a face (adv_mpdata_FCT_core.f90:103-115).
+// The fast variant's betas are already at most 1, and its form is a select.
+template <bool EXACT>
 __device__ __forceinline__ float limit(float u, float bin_r, float bout_l, float bin_l, float bout_r)
 {
-    if (u > 0.0f) return fminf(fminf(1.0f, bin_r), bout_l) * u;
-    if (u < 0.0f) return fminf(fminf(1.0f, bin_l), bout_r) * u;
-    return u;
+    if constexpr (EXACT) {
+        if (u > 0.0f) return fminf(fminf(1.0f, bin_r), bout_l) * u;
+        if (u < 0.0f) return fminf(fminf(1.0f, bin_l), bout_r) * u;
+        return u;
+    } else {
+        return (u > 0.0f ? fminf(bin_r, bout_l) : fminf(bin_l, bout_r)) * u;
+    }
 }
 
 // Per-cell limiter terms of one direction (the carried form of the FCT
@@ -239,21 +245,23 @@ __device__ __forceinline__ float2 cross_x(float2 v, float2 U, float2 ev, float2 
 
 }  // namespace opx
 
-template <bool EXACT, bool FCT>
-__global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_constant__ OnePassParams p)
+// One tile's march.  INT: the whole 64 x 32 plane lies inside the domain's
+// interior (x in [1, nx-2], y in [1, ny-2]), so no cell of the tile meets a
+// domain edge: the edge cases of the reference (boundary ring, first/last
+// cells of the limiter lines, faces that do not exist) drop out at compile
+// time.  Tiles that touch an edge take the general form.
+// bars: two mbarriers initialised once per CTA; ph[0], ph[1] count the
+// phases each has completed so far (a CTA may run several tiles), and are
+// advanced here by the phases this tile completes.  Returns false when a
+// TMA wait gave up (the flag in p.err is then set and the CTA must stop).
+template <bool EXACT, bool FCT, bool INT>
+__device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t *ph, const OnePassParams &p, int s,
+                                             int i0, int j0)
 {
     using namespace op;
     using namespace opx;
-    extern __shared__ float4 smem4[];
-    // planes start on 128-byte boundaries (TMA destinations); SMEM has the slack
-    float *sm = reinterpret_cast<float *>(smem4) + ((128u - (smem_u32(smem4) & 127u)) & 127u) / sizeof(float);
-    __shared__ __align__(8) uint64_t bars[2];
-
     const Geo g = p.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int s = blockIdx.x % p.nspecies;
-    const int tile = blockIdx.x / p.nspecies;
-    const int i0 = (tile % p.tiles_x) * TX, j0 = (tile / p.tiles_x) * TY;
     const int x0 = i0 - 4, y0 = j0 - 3;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int X = 2 * lane;
@@ -298,22 +306,25 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
         if (lg < nz) tma_load_3d(sG(lg), mG, x0, lg, y0, bar);
     };
     bool ok = true;
+    // The batch waited for at iteration t was issued on bars[t & 1]: the
+    // prologue's on bars[0], iteration t-1's otherwise.  Its phase number is
+    // the barrier's count at tile start plus the batches issued on it since.
+    const uint32_t b0 = ph[0], b1 = ph[1];
+    auto phase_of = [&](int t) -> uint32_t { return (t & 1) ? b1 + (uint32_t)(t - 1) / 2 : b0 + (uint32_t)t / 2; };
     // bounded wait on the batch of iteration t; on a timeout the whole CTA
     // stops after draining (with a bound) what it issued
     auto wait_batch = [&](int t) {
-        bool mine = mbar_wait_bounded(&bars[t & 1], (uint32_t)(t >> 1) & 1u, WAIT_LIMIT);
+        bool mine = mbar_wait_bounded(&bars[t & 1], phase_of(t) & 1u, WAIT_NS);
         if (!mine && threadIdx.x == 0) atomicExch(p.err, 1);
         ok = __syncthreads_and(mine ? 1 : 0) != 0;
         return ok;
     };
+    // every batch completes a phase (one arrival, possibly zero bytes): the
+    // prologue and the odd iterations on bars[0], the even ones on bars[1]
+    ph[0] = b0 + 1 + (uint32_t)(nz + 1) / 2;
+    ph[1] = b1 + (uint32_t)nz / 2 + 1;
 
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        mbar_fence_init();
-        tma_prefetch_map(mq);
-    }
-    __syncthreads();
+    if (threadIdx.x == 0) tma_prefetch_map(mq);
     if (threadIdx.x == 0) {
         // iteration 0 (and the level-0 donor pass before it) needs q0 at
         // levels 0..2, U_m, V_m and J*rho at 0..1 and W_m/dz at 0 (nz >= 3)
@@ -401,10 +412,12 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
             val = fma2(make_float2(-hd.x, -hd.y), rcp2(G), c);
             val = fma2(make_float2(-vdiv.x, -vdiv.y), rcp2(djr), val);
         }
-        const bool jin = j >= 0 && j < ny, jring = j == 0 || j == ny - 1;
-        float2 q1;
-        q1.x = !(inA && jin) ? 0.0f : ((jring || ia == 0 || ia == nx - 1) ? c.x : val.x);
-        q1.y = !(inB && jin) ? 0.0f : ((jring || ib == 0 || ib == nx - 1) ? c.y : val.y);
+        float2 q1 = val;
+        if (!INT) {
+            const bool jin = j >= 0 && j < ny, jring = j == 0 || j == ny - 1;
+            q1.x = !(inA && jin) ? 0.0f : ((jring || ia == 0 || ia == nx - 1) ? c.x : val.x);
+            q1.y = !(inB && jin) ? 0.0f : ((jring || ib == 0 || ib == nx - 1) ? c.y : val.y);
+        }
         st2(sQ1(L), Y, X, q1);
     };
 
@@ -459,8 +472,8 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                 u2[r] = v2[r] = w2[r] = fz[r] = zero2;
                 const int Y = rowY[r], j = rowj[r];
                 if (!(Y >= 2 && Y <= PH - 2)) continue;
-                const bool jin = j >= 0 && j < ny;
-                const bool jint = j > 0 && j < ny - 1;
+                const bool jin = INT || (j >= 0 && j < ny);
+                const bool jint = INT || (j > 0 && j < ny - 1);
                 // x faces ia, ib (west faces of the pair)
                 {
                     const float2 qc = ld2(Qc, Y, X), Ut = ld2(Uc, Y, X), Gt = ld2(Gcp, Y, X);
@@ -508,8 +521,11 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                             val = fma2(make_float2(-cu.x * ev.x, -cu.y * ev.y), eq, val);
                         }
                     }
-                    u2[r].x = (jin && ia >= 1 && ia <= nx - 1) ? val.x : 0.0f;
-                    u2[r].y = (jin && ib >= 1 && ib <= nx - 1) ? val.y : 0.0f;
+                    u2[r] = val;
+                    if (!INT) {
+                        u2[r].x = (jin && ia >= 1 && ia <= nx - 1) ? val.x : 0.0f;
+                        u2[r].y = (jin && ib >= 1 && ib <= nx - 1) ? val.y : 0.0f;
+                    }
                 }
                 // y face j (south faces of the pair)
                 {
@@ -518,7 +534,7 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                     const float2 Ut = ld2(Uc, Y, X), Us = ld2(Uc, Y - 1, X);
                     const float2 qcl = lft(qc), qcr = rgt(qc), qsl = lft(qs), qsr = rgt(qs);
                     const float2 Utr = rgt(Ut), Usr = rgt(Us);
-                    const bool xa = ia > 0 && ia < nx - 1, xb = ib > 0 && ib < nx - 1;
+                    const bool xa = INT || (ia > 0 && ia < nx - 1), xb = INT || (ib > 0 && ib < nx - 1);
                     float2 val;
                     if constexpr (EXACT) {
                         val = base_x(Vt, Gs, qc, qs);
@@ -564,9 +580,12 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                             val = fma2(make_float2(-cv.x * ev2.x, -cv.y * ev2.y), eq2, val);
                         }
                     }
-                    const bool fin = j >= 1 && j <= ny - 1;
-                    v2[r].x = (fin && inA) ? val.x : 0.0f;
-                    v2[r].y = (fin && inB) ? val.y : 0.0f;
+                    v2[r] = val;
+                    if (!INT) {
+                        const bool fin = j >= 1 && j <= ny - 1;
+                        v2[r].x = (fin && inA) ? val.x : 0.0f;
+                        v2[r].y = (fin && inB) ? val.y : 0.0f;
+                    }
                     st2(P(S_V2), Y, X, v2[r]);
                 }
                 // z face at the top of level t (columns inside the domain interior)
@@ -609,9 +628,12 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                         val = fma2(make_float2(-cw.x * ev2.x, -cw.y * ev2.y), eq2, val);
                         val = mul2(val, c_dz[r]);
                     }
-                    const bool jj = j >= 1 && j <= ny - 2;
-                    w2[r].x = (jj && ia >= 1 && ia <= nx - 2) ? val.x : 0.0f;
-                    w2[r].y = (jj && ib >= 1 && ib <= nx - 2) ? val.y : 0.0f;
+                    w2[r] = val;
+                    if (!INT) {
+                        const bool jj = j >= 1 && j <= ny - 2;
+                        w2[r].x = (jj && ia >= 1 && ia <= nx - 2) ? val.x : 0.0f;
+                        w2[r].y = (jj && ib >= 1 && ib <= nx - 2) ? val.y : 0.0f;
+                    }
                     fz[r] = flux<EXACT>(qc, qu, w2[r]);
                 }
             }
@@ -629,8 +651,8 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                 {
                     const float2 ur = rgt(u2[r]);
                     const float2 fl = flux<EXACT>(qcl, qc, u2[r]), fr = flux<EXACT>(qc, qcr, ur);
-                    const int pa = ia == 0 ? 1 : (ia == nx - 1 ? 2 : 0);
-                    const int pb = ib == 0 ? 1 : (ib == nx - 1 ? 2 : 0);
+                    const int pa = INT ? 0 : (ia == 0 ? 1 : (ia == nx - 1 ? 2 : 0));
+                    const int pb = INT ? 0 : (ib == 0 ? 1 : (ib == nx - 1 ? 2 : 0));
                     fct_cell<EXACT>(qcl.x, qc.x, qcr.x, q0l.x, q0c.x, q0r.x, fl.x, fr.x, pa, false, bxi[r].x, bxo[r].x);
                     fct_cell<EXACT>(qcl.y, qc.y, qcr.y, q0l.y, q0c.y, q0r.y, fl.y, fr.y, pb, false, bxi[r].y, bxo[r].y);
                 }
@@ -640,7 +662,7 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                     const float2 q0n = ld2(sq0(t), Y + 1, X), q0s = ld2(sq0(t), Y - 1, X);
                     const float2 vn = ld2(P(S_V2), Y + 1, X);
                     const float2 fl = flux<EXACT>(qs, qc, v2[r]), fr = flux<EXACT>(qc, qn, vn);
-                    const int pj = j == 0 ? 1 : (j == ny - 1 ? 2 : 0);
+                    const int pj = INT ? 0 : (j == 0 ? 1 : (j == ny - 1 ? 2 : 0));
                     fct_cell<EXACT>(qs.x, qc.x, qn.x, q0s.x, q0c.x, q0n.x, fl.x, fr.x, pj, false, byi[r].x, byo[r].x);
                     fct_cell<EXACT>(qs.y, qc.y, qn.y, q0s.y, q0c.y, q0n.y, fl.y, fr.y, pj, false, byi[r].y, byo[r].y);
                     st2(P(S_BYI), Y, X, byi[r]);
@@ -678,16 +700,16 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                 float2 vs = v2[r], vn = ld2(P(S_V2), Y + 1, X);
                 if (FCT) {
                     const float2 bil = lft(bxi[r]), bol = lft(bxo[r]), bir = rgt(bxi[r]), bor = rgt(bxo[r]);
-                    uw.x = limit(uw.x, bxi[r].x, bol.x, bil.x, bxo[r].x);
-                    uw.y = limit(uw.y, bxi[r].y, bxo[r].x, bxi[r].x, bxo[r].y);
+                    uw.x = limit<EXACT>(uw.x, bxi[r].x, bol.x, bil.x, bxo[r].x);
+                    uw.y = limit<EXACT>(uw.y, bxi[r].y, bxo[r].x, bxi[r].x, bxo[r].y);
                     ue.x = uw.y;
-                    ue.y = limit(ue.y, bir.y, bxo[r].y, bxi[r].y, bor.y);
+                    ue.y = limit<EXACT>(ue.y, bir.y, bxo[r].y, bxi[r].y, bor.y);
                     const float2 bis = ld2(P(S_BYI), Y - 1, X), bos = ld2(P(S_BYO), Y - 1, X);
                     const float2 bin = ld2(P(S_BYI), Y + 1, X), bon = ld2(P(S_BYO), Y + 1, X);
-                    vs.x = limit(vs.x, byi[r].x, bos.x, bis.x, byo[r].x);
-                    vs.y = limit(vs.y, byi[r].y, bos.y, bis.y, byo[r].y);
-                    vn.x = limit(vn.x, bin.x, byo[r].x, byi[r].x, bon.x);
-                    vn.y = limit(vn.y, bin.y, byo[r].y, byi[r].y, bon.y);
+                    vs.x = limit<EXACT>(vs.x, byi[r].x, bos.x, bis.x, byo[r].x);
+                    vs.y = limit<EXACT>(vs.y, byi[r].y, bos.y, bis.y, byo[r].y);
+                    vn.x = limit<EXACT>(vn.x, bin.x, byo[r].x, byi[r].x, bon.x);
+                    vn.y = limit<EXACT>(vn.y, bin.y, byo[r].y, byi[r].y, bon.y);
                 }
                 const float2 fe = flux<EXACT>(qc, qcr, ue), fw = flux<EXACT>(qcl, qc, uw);
                 const float2 f3 = flux<EXACT>(qc, qn, vn), f4 = flux<EXACT>(qs, qc, vs);
@@ -698,8 +720,8 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                 // limited w2 at the top of level t-1
                 float2 w = r_w2[r];
                 if (FCT && t >= 1) {
-                    w.x = limit(w.x, bzi[r].x, r_bzo[r].x, r_bzi[r].x, bzo[r].x);
-                    w.y = limit(w.y, bzi[r].y, r_bzo[r].y, r_bzi[r].y, bzo[r].y);
+                    w.x = limit<EXACT>(w.x, bzi[r].x, r_bzo[r].x, r_bzi[r].x, bzo[r].x);
+                    w.y = limit<EXACT>(w.y, bzi[r].y, r_bzo[r].y, r_bzi[r].y, bzo[r].y);
                 }
                 n_w2l = w;
             }
@@ -727,13 +749,16 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
                     else vd = sub2(mul2(qc, wtop), flux_f(qdd, qc, wbot));
                     val = fma2(make_float2(-vd.x, -vd.y), rcp2(djr), val);
                 }
-                const bool jin = j >= 0 && j < ny;
-                const bool jring = j == 0 || j == ny - 1;
-                const bool oa = jin && inA && X >= 4 && X < 4 + TX;
-                const bool ob = jin && inB && X + 1 >= 4 && X + 1 < 4 + TX;
-                const float2 q0L = ld2(sq0(L), Y, X);
-                const float va = (jring || ia == 0 || ia == nx - 1) ? q0L.x : val.x;
-                const float vb = (jring || ib == 0 || ib == nx - 1) ? q0L.y : val.y;
+                const bool jin = INT || (j >= 0 && j < ny);
+                const bool jring = !INT && (j == 0 || j == ny - 1);
+                const bool oa = jin && (INT || inA) && X >= 4 && X < 4 + TX;
+                const bool ob = jin && (INT || inB) && X + 1 >= 4 && X + 1 < 4 + TX;
+                float va = val.x, vb = val.y;
+                if (!INT) {
+                    const float2 q0L = ld2(sq0(L), Y, X);
+                    va = (jring || ia == 0 || ia == nx - 1) ? q0L.x : val.x;
+                    vb = (jring || ib == 0 || ib == nx - 1) ? q0L.y : val.y;
+                }
                 if (oa || ob) {
                     // ia is even and rows start on 16-byte boundaries: the pair is 8-byte aligned
                     float *dst = outg + ix(g, 0, L, j);
@@ -755,13 +780,93 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
             r_wm[r] = c_wmn[r];
         }
     }
-    return;
+    return true;
 
 drain:
-    // a wait gave up: wait (bounded) for both batches so no copy is left in
-    // flight into this CTA's shared memory, then stop
-    mbar_wait_bounded(&bars[0], 0, WAIT_LIMIT);
-    mbar_wait_bounded(&bars[1], 0, WAIT_LIMIT);
+    // a wait gave up: wait (bounded) for both barriers' latest batches so
+    // no copy is left in flight into this CTA's shared memory, then stop
+    mbar_wait_bounded(&bars[0], (ph[0] - 1) & 1u, WAIT_NS);
+    mbar_wait_bounded(&bars[1], (ph[1] - 1) & 1u, WAIT_NS);
+    return false;
+}
+
+// Barrier set-up, once per CTA.
+__device__ __forceinline__ void onepass_init_bars(uint64_t *bars, uint32_t *ph)
+{
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    ph[0] = ph[1] = 0;
+    __syncthreads();
+}
+
+// Whether a tile's whole plane lies inside the domain interior.
+__device__ __forceinline__ bool onepass_interior(const Geo &g, int i0, int j0)
+{
+    return i0 - 4 >= 1 && i0 - 4 + op::PW - 1 <= g.nx - 2 && j0 - 3 >= 1 && j0 - 3 + op::PH - 1 <= g.ny - 2;
+}
+
+template <bool EXACT, bool FCT>
+__global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_constant__ OnePassParams p)
+{
+    using namespace op;
+    extern __shared__ float4 smem4[];
+    // planes start on 128-byte boundaries (TMA destinations); SMEM has the slack
+    float *sm = reinterpret_cast<float *>(smem4) + ((128u - (smem_u32(smem4) & 127u)) & 127u) / sizeof(float);
+    __shared__ __align__(8) uint64_t bars[2];
+    const int s = blockIdx.x % p.nspecies;
+    const int tile = blockIdx.x / p.nspecies;
+    const int i0 = (tile % p.tiles_x) * TX, j0 = (tile / p.tiles_x) * TY;
+    __shared__ int stop;
+    if (threadIdx.x == 0) stop = *reinterpret_cast<volatile const int *>(p.err);
+    __syncthreads();
+    if (stop) return;   // an earlier tile of this launch gave up on a TMA wait: stop (the whole CTA)
+    uint32_t ph[2];
+    onepass_init_bars(bars, ph);
+    if (onepass_interior(p.g, i0, j0)) onepass_tile<EXACT, FCT, true>(sm, bars, ph, p, s, i0, j0);
+    else onepass_tile<EXACT, FCT, false>(sm, bars, ph, p, s, i0, j0);
+}
+
+// Batched form: persistent CTAs (one per SM) pull (member, species, i0, j0)
+// items from a work list with an atomic counter; params[member] holds that
+// member's descriptors, pointers and geometry for the current buffer parity.
+template <bool EXACT, bool FCT>
+__global__ void __launch_bounds__(op::NT, 1)
+    k_batch_onepass(const OnePassParams *__restrict__ params, const int4 *__restrict__ items, int n_items,
+                    int *__restrict__ counter)
+{
+    extern __shared__ float4 smem4[];
+    float *sm = reinterpret_cast<float *>(smem4) + ((128u - (smem_u32(smem4) & 127u)) & 127u) / sizeof(float);
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int next;
+    // the member's parameters, staged in shared memory so that the tile code
+    // reads them from there rather than holding them in registers
+    __shared__ __align__(16) OnePassParams sp;
+    constexpr int PW4 = (int)(sizeof(OnePassParams) / sizeof(int));
+    static_assert(sizeof(OnePassParams) % sizeof(int) == 0, "parameter block is whole words");
+    uint32_t ph[2];
+    onepass_init_bars(bars, ph);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            // stop handing out work once any tile has given up on a TMA wait
+            const int failed = *reinterpret_cast<volatile const int *>(params[0].err);
+            next = failed ? n_items : atomicAdd(counter, 1);
+        }
+        __syncthreads();
+        const int it = next;
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const int *src = reinterpret_cast<const int *>(params + w.x);
+        for (int q = threadIdx.x; q < PW4; q += blockDim.x) reinterpret_cast<int *>(&sp)[q] = src[q];
+        __syncthreads();
+        bool fine;
+        if (onepass_interior(sp.g, w.z, w.w)) fine = onepass_tile<EXACT, FCT, true>(sm, bars, ph, sp, w.y, w.z, w.w);
+        else fine = onepass_tile<EXACT, FCT, false>(sm, bars, ph, sp, w.y, w.z, w.w);
+        if (!fine) break;  // the barriers' phases are no longer known: this CTA stops
+        __syncthreads();   // every thread is done with the planes and parameters before the next tile
+    }
 }
 
 }  // namespace icar

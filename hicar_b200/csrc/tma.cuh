@@ -42,14 +42,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Wait for the phase of the given parity, at most `limit` polls (each poll
-// may suspend the thread for a short hardware-chosen time).  Returns false
-// when the limit was reached.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit)
+__device__ __forceinline__ uint64_t global_ns()
 {
-    for (uint32_t n = 0; n < limit; n++)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+
+// Wait for the phase of the given parity for at most `limit_ns` nanoseconds
+// of wall time.  Returns false when the limit was reached.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int n = 0; n < 64; n++)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
 }
 
 // 3-D tiled TMA load of one box into shared memory (coordinates innermost

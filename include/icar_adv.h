@@ -300,6 +300,13 @@ int icar_adv_batch_sync(icar_adv_batch_t *b);
 /* Bounded wait for the batch's steps; ICAR_ADV_TIMEOUT after timeout_s. */
 int icar_adv_batch_sync_timeout(icar_adv_batch_t *b, double timeout_s);
 int icar_adv_batch_set_stream(icar_adv_batch_t *b, void *cuda_stream);
+/* MPDATA kernels of the batch's step (no reference counterpart): 0 = the
+ * donor-cell kernel then the fused correction (default), 2 = the single-pass
+ * kernel with the reference's FP32 arithmetic (bit-identical results), 3 =
+ * the single-pass kernel with fast arithmetic (hardware reciprocal
+ * approximation and fused multiply-adds; results within the tolerance
+ * stated with icar_adv_set_path). */
+int icar_adv_batch_set_path(icar_adv_batch_t *b, int32_t path);
 /* Event timing of every step launched while enabled; reading synchronises. */
 int icar_adv_batch_profile(icar_adv_batch_t *b, int32_t enable);
 int icar_adv_batch_profile_read(icar_adv_batch_t *b, double *step_ms, int64_t *steps, int64_t *kernels_per_step,
@@ -370,8 +377,22 @@ int icar_adv_set_tile_shape(icar_adv_t *h, int32_t shape);
 int icar_adv_set_species_group(icar_adv_t *h, int32_t group);
 int icar_adv_tile_shapes(int32_t *n_shapes, int32_t *rows);
 
-/* Kernel selection for testing: 0 = fused MPDATA kernel where it applies
- * (default), 1 = the staged one-stage-per-kernel path. */
+/* Kernel selection (no reference counterpart).  MPDATA order 2 without
+ * RK3 runs as:
+ *   0  the donor-cell kernel then the fused correction kernel (default;
+ *      the reference's FP32 arithmetic, bit-identical results);
+ *   1  one kernel per reference stage (any mpdata_order; bit-identical);
+ *   2  the single-pass kernel (donor-cell pass, pseudo-velocities, limiter
+ *      and corrective pass in one launch for every species; bit-identical);
+ *   3  the single-pass kernel with fast arithmetic: hardware reciprocal
+ *      approximation, fused multiply-adds and reassociated pair sums.  Not
+ *      bit-identical; tolerance as tested: max relative error (floor
+ *      1e-6 * max|q|) <= 1e-5 after one step and <= 1e-4 after 100 steps on
+ *      a smooth tracer, error against an FP64 evaluation within 5x the
+ *      reference FP32 arithmetic's own, 99.9 % of cells within 1e-5 of the
+ *      FP32 result, and mass conserved to 2e-6.
+ * Other schemes and orders ignore 2 and 3 (the standard scheme always runs
+ * its fused kernels on 0, 2 and 3). */
 int icar_adv_set_path(icar_adv_t *h, int32_t path);
 
 #ifdef __cplusplus

@@ -121,3 +121,60 @@ def test_batch_rejects_ineligible_members():
         b.add(d, c.dt)
     b.close()
     d.close()
+
+
+@pytest.mark.parametrize("path", [2, 3])
+def test_batch_single_pass_kernel(oracle_lib, path):
+    """The batched step on the single-pass kernel (a persistent launch over
+    every member's 56 x 26 tiles): bit-identical to the oracle and to each
+    member stepped alone with the bit-exact arithmetic (path 2); within the
+    fast variant's tolerance with fast arithmetic (path 3), and still
+    identical to the same member stepped alone on the same kernel."""
+    shapes = [(40, 36, 12), (67, 30, 20), (129, 61, 9), (100, 64, 7), (33, 33, 25)]
+    cases = make_members(shapes, seed0=60)
+    forc = [forcing_for(c, i) if i % 2 == 0 else None for i, c in enumerate(cases)]
+    b = Batch()
+    b.set_path(path)
+    doms = []
+    for c, f in zip(cases, forc):
+        d = Domain.from_case(c)
+        if f is not None:
+            for k in c.species:
+                d.set_forcing(k, f[k][0], f[k][1])
+        adv_init(d, Options())
+        b.add(d, c.dt)
+        doms.append(d)
+    nsteps = 5
+    for _ in range(nsteps):
+        b.step()
+    b.sync()
+    O = oracle_lib
+    for c, d, f in zip(cases, doms, forc):
+        got = {k: d.fetch(k).copy() for k in c.species}
+        # the same member alone on the same kernel
+        a = Domain.from_case(c)
+        if f is not None:
+            for k in c.species:
+                a.set_forcing(k, f[k][0], f[k][1])
+        adv_init(a, Options())
+        a.set_path(path)
+        for _ in range(nsteps):
+            step(a, Options(), c.dt)
+        alone = {k: a.fetch(k).copy() for k in c.species}
+        a.close()
+        for k in c.species:
+            assert np.array_equal(got[k], alone[k]), ("alone", path, c.nx, c.ny, c.nz, k)
+        if f is None:
+            ref = O.run_steps(c, O.make_opts(), c.dt, nsteps)
+        else:
+            flt = O.init_relax_filters(c.nx, c.ny, 2)
+            ref = O.run_steps(c, O.make_opts(), c.dt, nsteps, forcing=f, filter2d=flt)
+        for k in c.species:
+            if path == 2:
+                assert np.array_equal(got[k], ref[k]), ("oracle", c.nx, c.ny, c.nz, k)
+            else:
+                scale = float(np.abs(ref[k]).max()) or 1.0
+                assert float(np.abs(got[k].astype(np.float64) - ref[k]).max()) / scale <= 1e-5, (c.nx, k)
+    b.close()
+    for d in doms:
+        d.close()
