@@ -49,16 +49,19 @@ def parse():
                    choices=["full_species", "plain_c1", "mid_species", "ensemble", "served", "large", "wind", "mp",
                             "std"])
     p.add_argument("--serve-rate", type=float, default=20.0)
-    p.add_argument("--serve-duration", type=float, default=6.0)
+    p.add_argument("--serve-duration", type=float, default=20.0)
     p.add_argument("--serve-steps-scale", type=float, default=0.1)
     p.add_argument("--members", type=int, default=64, help="ensemble size (ensemble workload)")
     p.add_argument("--tile-shape", default="auto", choices=["auto", "0", "1", "2", "3"],
                    help="fused-kernel tile shape 0..3 (8/15/24/31 rows), or auto: chosen by hicar_b200.autotune")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--staged", action="store_true", help="use the staged kernels instead of the fused one")
-    p.add_argument("--kernel", default="two-pass", choices=["two-pass", "single-pass", "single-pass-fast"],
+    p.add_argument("--kernel", default="single-pass-fast", choices=["two-pass", "single-pass", "single-pass-fast"],
                    help="MPDATA kernels: the donor-cell kernel then the fused correction (two-pass), or the "
                         "single-pass kernel with bit-exact or fast arithmetic")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the sub-records of the default line (bit-exact kernels, drift, batched, served)")
+    p.add_argument("--drift-steps", type=int, default=200, help="steps of the drift record (blocks of 20)")
     p.add_argument("--quick", action="store_true",
                    help="timed region only (no e2e, no CPU baseline): the profiling run")
     return p.parse_args()
@@ -231,12 +234,10 @@ def run_b200(args):
     for k, q in case.species.items():
         d.set_forcing(k, q.copy(), None)            # fixed inflow: forcing = initial state, dqdt = 0
     adv_init(d, opts)
-    if args.staged:
-        d.use_staged_kernels(True)
-    launch = set_launch_shape(d, args)
-    if not args.staged and args.kernel != "two-pass":
-        d.use_single_pass(fast=args.kernel == "single-pass-fast")
-        launch = {"kernel": args.kernel, "tile": "56 x 26 columns per CTA, 16 warps"}
+    path = 1 if args.staged else KERNEL_PATH[args.kernel]
+    launch = set_launch_shape(d, args) if path == 0 else (
+        {"kernel": "staged"} if path == 1 else {"kernel": args.kernel, "tile": "56 x 26 columns per CTA, 16 warps"})
+    d.set_path(path)
     # a dedicated stream: the library and the timing events share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -250,6 +251,19 @@ def run_b200(args):
     def barrier():
         R.barrier(rk)
 
+    def timed_steps(n):
+        """Device time (ms) of n steps, CUDA events on the library's stream."""
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return e0.elapsed_time(e1)
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -259,35 +273,29 @@ def run_b200(args):
     clocks.start()
     time.sleep(0.4)
     L.check(lib.icar_adv_profile(h, 1), h)
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms = e0.elapsed_time(e1)
+    ms = timed_steps(args.steps)
     clk = clocks.stop()
     kms, klaunch, alll, passes = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
     L.check(lib.icar_adv_profile_read(h, C.byref(kms), C.byref(klaunch), C.byref(alll), C.byref(passes)), h)
     cms, claunch = C.c_double(), C.c_int64()
     L.check(lib.icar_adv_profile_read_correction(h, C.byref(cms), C.byref(claunch)), h)
     L.check(lib.icar_adv_profile(h, 0), h)
+    L.check(lib.icar_adv_sync(h), h)
     ms_max = R.max_over_ranks(rk, ms)
     value = R.whole_job_rate(cells * S * args.steps, world, ms_max / 1e3)
 
-    # ---- roofline of the species kernels ------------------------------
+    # ---- roofline of the dominant kernel and of the whole advect call ---
     from hicar_b200 import roofline
     step_rl = roofline.species_pass(case.nx, case.ny, case.nz, S, kms.value, passes.value)
-    if claunch.value > 0:
+    if claunch.value > 0 and path >= 2:
+        rl = roofline.single_pass_kernel(case.nx, case.ny, case.nz, S, cms.value, claunch.value)
+        rl["advect_call"] = step_rl
+    elif claunch.value > 0:
         rl = roofline.correction_kernel(case.nx, case.ny, case.nz, S, cms.value, claunch.value)
         rl["advect_call"] = step_rl
     else:                                       # staged path: the whole advect call
         rl = step_rl
 
-    # ---- end to end through the C ABI with pinned host buffers ---------
     if args.quick:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "quick": True,
@@ -295,6 +303,32 @@ def run_b200(args):
         d.close()
         R.finalize(rk)
         return
+
+    extras = {}
+    if not args.no_extras:
+        # ---- the bit-exact kernels on the same workload (same state) ----
+        if path != 0:
+            d.set_path(0)
+            for _ in range(2):
+                step()
+            ems = R.max_over_ranks(rk, timed_steps(args.steps))
+            extras["exact"] = {
+                "value": R.whole_job_rate(cells * S * args.steps, world, ems / 1e3), "unit": UNIT,
+                "ms_per_step": ems / args.steps, "steps": args.steps,
+                "kernel": "two-pass (donor-cell kernel + fused correction), the reference's FP32 arithmetic, "
+                          "bit-identical to the oracle"}
+            d.set_path(path)
+        # ---- drift: the step cost as the fields evolve, from the initial state
+        for k, q in case.species.items():
+            d.upload(k, q)
+        blocks, nb = [], max(1, args.drift_steps // 20)
+        for _ in range(nb):
+            blocks.append(R.max_over_ranks(rk, timed_steps(20)) / 20)
+        extras["drift"] = {"steps": 20 * nb, "block": 20, "ms_per_step_first": blocks[0],
+                           "ms_per_step_last": blocks[-1], "ms_per_step_blocks": blocks,
+                           "from": "the initial state", "kernel": args.kernel if path >= 2 else "two-pass"}
+
+    # ---- end to end through the C ABI with pinned host buffers ---------
     host = {k: torch.from_numpy(v.copy()).pin_memory() for k, v in case.species.items()}
     ids = {k: L.SPECIES_IDS[k] for k in case.species}
     e2e_steps = max(3, min(args.steps, 20))
@@ -325,6 +359,15 @@ def run_b200(args):
     e2e_val = R.whole_job_rate(cells * S * e2e_steps, world, e2e_s)
     e2e_pf = R.whole_job_rate(cells * S * e2e_steps, world, e2e_time(e2e_step_per_field))
     bytes_io = cells * S * 4
+    d.close()
+
+    if not args.no_extras and world == 1:
+        # ---- the metric's batched and served forms (config 3 and 4) ------
+        ens = ensemble_core(args, rk, args.kernel if path >= 2 else "two-pass", want_e2e=False, want_cpu=False)
+        ens["workload"] = ENSEMBLE_DESC
+        extras["batched"] = ens
+        srv = served_core(args, args.kernel if path >= 2 else "two-pass")
+        extras["served"] = {"workload": srv["workload"], **srv["report"], "clocks": srv["clocks"]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -336,12 +379,16 @@ def run_b200(args):
                          f"{el:.1f} s (C restatement, OpenMP over all host threads)"}
 
     if rank == 0:
+        arith = ("fast: hardware reciprocal approximation, fused multiply-adds; within the tested tolerance of "
+                 "the reference's FP32 results (see icar_adv_set_path)" if path == 3 else
+                 "the reference's FP32 arithmetic, bit-identical to the oracle")
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
                        "kernel_path": "staged" if args.staged else args.kernel,
+                       "arithmetic": arith,
                        "launch_shape": launch,
                        "l2": "inputs larger than L2 (12 fields x 42 MB per domain)",
                        "parallelism": f"replicas x{world}"},
@@ -353,8 +400,8 @@ def run_b200(args):
             "gpu_launches": int(alll.value),
             "clocks": clk,
         }
+        out.update(extras)
         print(json.dumps(out), flush=True)
-    d.close()
     R.finalize(rk)
 
 
@@ -708,18 +755,18 @@ def make_ensemble(n: int, seed: int):
         return list(ex.map(_member, jobs))
 
 
-def run_ensemble(args):
+def ensemble_core(args, rk, kernel: str, want_e2e: bool, want_cpu: bool) -> dict:
+    """The config-3 ensemble on this rank: plain (one member after another,
+    each with its own launches) against batched (one step for every member,
+    CUDA graph), both on the chosen kernels.  Returns the measurements."""
     import torch
 
     from hicar_b200 import _lib as L, replicas as R, roofline
     from hicar_b200.advection import Domain, Options, adv_init
     from hicar_b200.batch import Batch
 
-    rk = R.from_env()
     world, rank, local = rk.world, rk.rank, rk.local
     cases = make_ensemble(args.members, R.replica_seed(7, rk))
-    torch.cuda.set_device(local)
-    R.init(rk, "nccl", timeout_s=600)
     lib = L.load()
     opts = Options()
     stream = torch.cuda.Stream()
@@ -731,15 +778,12 @@ def run_ensemble(args):
             d.set_forcing(k, q, None)           # fixed inflow boundaries
         adv_init(d, opts)
         L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(stream.cuda_stream)), d.handle)
-        d.set_path(KERNEL_PATH[args.kernel])
+        d.set_path(KERNEL_PATH[kernel])
         doms.append(d)
     cs_step = sum(c.cells() * len(c.species) for c in cases)
 
-    def barrier():
-        R.barrier(rk)
-
     def timed(fn, steps):
-        barrier()
+        R.barrier(rk)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -747,7 +791,7 @@ def run_ensemble(args):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        barrier()
+        R.barrier(rk)
         return R.max_over_ranks(rk, e0.elapsed_time(e1))
 
     # ---- plain: one domain per launch sequence, members one after another
@@ -764,11 +808,11 @@ def run_ensemble(args):
     # ---- batched: every member in one graph launch per step
     b = Batch(device=local)
     b.set_stream(stream.cuda_stream)
-    b.set_path(KERNEL_PATH[args.kernel])
+    b.set_path(KERNEL_PATH[kernel])
     for d, c in zip(doms, cases):
         b.add(d, c.dt)
     shape = 1
-    if args.kernel != "two-pass":
+    if kernel != "two-pass":
         pass                                    # the single-pass kernel has one tile shape
     elif args.tile_shape == "auto":
         from hicar_b200 import autotune
@@ -786,6 +830,7 @@ def run_ensemble(args):
     clk = clocks.stop()
     prof = b.profile_read()
     b.profile(False)
+    b.sync()
     value = R.whole_job_rate(cs_step * args.steps, world, ms / 1e3)
     bytes_step = sum(c.cells() * (8 * len(c.species) + 32) for c in cases)
     peak, kind = roofline.hbm_peak()
@@ -794,96 +839,102 @@ def run_ensemble(args):
     rl = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
           "traffic": None, "peak_kind": kind, "algorithmic_bytes_per_launch": bytes_step, "launch_ms": step_ms,
           "bytes_model": "8 + 32/S B per cell-species; one launch = one batched step (graph)"}
-    if args.quick:
-        if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "quick": True, "plain_value": plain_value,
-                              "ms_per_step": ms / args.steps, "roofline": rl}), flush=True)
-        b.close()
-        for d in doms:
-            d.close()
-        R.finalize(rk)
-        return
+    out = {"value": value, "ms_per_step": ms / args.steps, "steps": args.steps, "cell_species_per_step": cs_step,
+           "members": len(cases), "kernel": kernel,
+           "tile_shape_rows": [8, 15, 24, 31][shape] if kernel == "two-pass" else 26,
+           "plain": {"value": plain_value, "steps": plain_steps, "ms_per_step": plain_ms / plain_steps,
+                     "launches_per_step": len(cases) * (3 if kernel != "two-pass" else 4)},
+           "batched_over_plain": value / plain_value, "roofline": rl,
+           "gpu_launches": int(prof["kernels_per_step"] * prof["steps"]), "clocks": clk}
 
-    # ---- end to end: host buffers in and out of every member every step
-    host = [{k: torch.from_numpy(v.copy()).pin_memory() for k, v in c.species.items()} for c in cases]
+    if want_e2e:
+        # host buffers in and out of every member every step
+        host = [{k: torch.from_numpy(v.copy()).pin_memory() for k, v in c.species.items()} for c in cases]
 
-    def e2e_step():
-        for d, hb in zip(doms, host):
-            for k, tns in hb.items():
-                L.check(lib.icar_adv_set_field(d.handle, L.SPECIES_IDS[k], C.c_void_p(tns.data_ptr()), None), d.handle)
-        b.step()
-        for d, hb in zip(doms, host):
-            for k, tns in hb.items():
-                L.check(lib.icar_adv_get_field(d.handle, L.SPECIES_IDS[k], C.c_void_p(tns.data_ptr()), None), d.handle)
+        def e2e_step():
+            for d, hb in zip(doms, host):
+                for k, tns in hb.items():
+                    L.check(lib.icar_adv_set_field(d.handle, L.SPECIES_IDS[k], C.c_void_p(tns.data_ptr()), None),
+                            d.handle)
+            b.step()
+            for d, hb in zip(doms, host):
+                for k, tns in hb.items():
+                    L.check(lib.icar_adv_get_field(d.handle, L.SPECIES_IDS[k], C.c_void_p(tns.data_ptr()), None),
+                            d.handle)
 
-    e2e_step()
-    barrier()
-    torch.cuda.synchronize()
-    e2e_steps = 3
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
         e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = R.max_over_ranks(rk, time.perf_counter() - t0)
-    e2e_val = R.whole_job_rate(cs_step * e2e_steps, world, e2e_s)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        R.barrier(rk)
+        torch.cuda.synchronize()
+        e2e_steps = 3
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = R.max_over_ranks(rk, time.perf_counter() - t0)
+        out["e2e"] = {"value": R.whole_job_rate(cs_step * e2e_steps, world, e2e_s), "unit": UNIT,
+                      "h2d_bytes_per_step": cs_step * 4, "d2h_bytes_per_step": cs_step * 4, "steps": e2e_steps}
+    if want_cpu and rank == 0 and world == 1:
         threads = os.cpu_count() or 1
         big = max(cases, key=lambda c: c.cells())
         rate, el, nst = cpu_rate(big.copy(), threads)
-        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"largest member {big.nx}x{big.ny}x{big.nz}, 12 fields, {nst} steps, {el:.1f} s "
-                         f"(C restatement, OpenMP over all host threads)"}
-    if rank == 0:
-        out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": ENSEMBLE_DESC, "members": len(cases), "cell_species_per_step": cs_step,
-                       "scheme": "MPDATA order 2 + FCT, relaxation boundary update",
-                       "kernel": args.kernel,
-                       "tile_shape_rows": [8, 16, 24, 32][shape] if args.kernel == "two-pass" else 26,
-                       "tile_shape_chosen_by": ("autotune cost model" if args.tile_shape == "auto" else "--tile-shape")
-                       if args.kernel == "two-pass" else "fixed 56 x 26 tiles",
-                       "l2": "inputs larger than L2 (~6 GB of species per step)",
-                       "parallelism": f"replicas x{world}"},
-            "plain": {"value": plain_value, "steps": plain_steps, "ms_per_step": plain_ms / plain_steps,
-                      "launches_per_step": sum(len(c.species) + 3 for c in cases)},
-            "batched_over_plain": value / plain_value,
-            "roofline": rl,
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": cs_step * 4, "d2h_bytes_per_step": cs_step * 4,
-                    "steps": e2e_steps},
-            "gpu_launches": int(prof["kernels_per_step"] * prof["steps"]),
-            "clocks": clk,
-        }
-        print(json.dumps(out), flush=True)
+        out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"largest member {big.nx}x{big.ny}x{big.nz}, 12 fields, {nst} steps, "
+                                         f"{el:.1f} s (C restatement, OpenMP over all host threads)"}
     b.close()
     for d in doms:
         d.close()
+    return out
+
+
+def run_ensemble(args):
+    from hicar_b200 import replicas as R
+    import torch
+
+    rk = R.from_env()
+    torch.cuda.set_device(rk.local)
+    R.init(rk, "nccl", timeout_s=600)
+    r = ensemble_core(args, rk, args.kernel, want_e2e=not args.quick, want_cpu=not (args.quick or args.no_cpu_baseline))
+    if rk.rank == 0:
+        if args.quick:
+            print(json.dumps({"metric": METRIC, "value": r["value"], "unit": UNIT, "quick": True,
+                              "plain_value": r["plain"]["value"], "ms_per_step": r["ms_per_step"],
+                              "roofline": r["roofline"]}), flush=True)
+        else:
+            out = {
+                "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": rk.world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": ENSEMBLE_DESC, "members": r["members"],
+                           "cell_species_per_step": r["cell_species_per_step"],
+                           "scheme": "MPDATA order 2 + FCT, relaxation boundary update", "kernel": r["kernel"],
+                           "tile_shape_rows": r["tile_shape_rows"],
+                           "l2": "inputs larger than L2 (~6 GB of species per step)",
+                           "parallelism": f"replicas x{rk.world}"},
+                "plain": r["plain"], "batched_over_plain": r["batched_over_plain"], "roofline": r["roofline"],
+                "cpu_baseline": r.get("cpu_baseline"), "e2e": r.get("e2e"), "gpu_launches": r["gpu_launches"],
+                "clocks": r["clocks"],
+            }
+            print(json.dumps(out), flush=True)
     R.finalize(rk)
 
 
 # -------------------------------------------------------------- served
-def run_served(args):
+def served_core(args, kernel: str) -> dict:
     """Poisson arrivals of downscaling requests into the continuous-batching
     server (config 4's size distributions; the arrival window and the step
     counts are scaled by --serve-duration and --serve-steps-scale so a run
-    fits in minutes)."""
+    fits in minutes).  Returns the server's report and the workload."""
     import torch
-    from hicar_b200 import replicas as R
     from hicar_b200.serve import Server, poisson_requests
 
-    if not R.from_env().is_root:
-        return                                   # one server on one GPU: the other ranks have no work
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     smin, smax = int(round(50 * args.serve_steps_scale)), int(round(500 * args.serve_steps_scale))
     reqs = poisson_requests(args.serve_rate, args.serve_duration, seed=11, steps=(max(1, smin), max(1, smax)))
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    srv = Server(device=local, budget_bytes=150e9, keep_results=False, stream=stream.cuda_stream)
+    srv = Server(device=local, budget_bytes=150e9, keep_results=False, stream=stream.cuda_stream,
+                 path=KERNEL_PATH[kernel])
     for r in reqs:
         srv.submit(r)
     clocks = ClockSampler(local)
@@ -893,13 +944,23 @@ def run_served(args):
     clk = clocks.stop()
     rep = srv.report()
     srv.close()
+    desc = (f"served requests: Poisson {args.serve_rate} req/s for {args.serve_duration} s (config 4: 120 s), "
+            f"area lognormal median 256^2 (sides 64..1024), nz U[20,60], 12 fields, steps U[{smin},{smax}] "
+            f"(config 4: U[50,500], scaled by {args.serve_steps_scale}), HBM admission budget 150 GB, "
+            f"kernel {kernel}")
+    return {"report": rep, "workload": desc, "clocks": clk}
+
+
+def run_served(args):
+    from hicar_b200 import replicas as R
+    if not R.from_env().is_root:
+        return                                   # one server on one GPU: the other ranks have no work
+    r = served_core(args, args.kernel)
+    rep = r["report"]
     print(json.dumps({
         "metric": METRIC + " (served)", "value": rep.get("throughput_cell_species_per_s"), "unit": UNIT,
         "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"served requests: Poisson {args.serve_rate} req/s for {args.serve_duration} s, "
-                               f"area lognormal median 256^2 (sides 64..1024), nz U[20,60], 12 fields, "
-                               f"steps U[{smin},{smax}], HBM admission budget 150 GB"},
-        "serving": rep, "clocks": clk}), flush=True)
+        "config": {"workload": r["workload"]}, "serving": rep, "clocks": r["clocks"]}), flush=True)
 
 
 def main():

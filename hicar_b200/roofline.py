@@ -8,7 +8,13 @@ once per step (32 B per cell), shared by the S species:
 One advect call (all S species) therefore moves cells * (8*S + 32)
 algorithmic bytes.  advection_dz is one value per level and is not counted.
 
-The dominant kernel of the step, the fused correction kernel (k_mp_corr),
+The single-pass kernel (k_mpdata_onepass) reads each species once and
+writes it once (8 B per cell-species) and reads seven species-independent
+fields once (U_m, V_m, W_m/dz and J*rho through TMA, W_m, dz*J*rho and dz by
+plain loads: 28 B per cell):
+    8 + 28/S bytes per cell-species  (10.33 B at S=12).
+
+The dominant kernel of the two-kernel form, the fused correction kernel (k_mp_corr),
 reads q0 and q1 and writes the new state of every species (12 B per
 cell-species) and reads six species-independent fields once (U_m, V_m,
 W_m/dz, J*rho, dz*J*rho and dz: 24 B per cell):
@@ -77,4 +83,29 @@ def correction_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launch
         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per cell-species of a "
                            "256x256x40x12 launch, scaled to this launch by cell-species")
         if CORR_DRAM_BYTES_PER_CS else None,
+    }
+
+
+# DRAM bytes (read + write) per cell-species of one k_mpdata_onepass launch
+# (fast variant, FCT on), from an ncu capture of a 256x256x40, 12-species
+# launch: 227.97 MB read + 103.27 MB written for 31.46 M cell-species.
+ONEPASS_DRAM_BYTES_PER_CS = (227.970048e6 + 103.272448e6) / (256 * 256 * 40 * 12)
+
+
+def single_pass_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launches: int) -> dict:
+    """Roofline entry for the single-pass kernel alone (all S species of one
+    advect call per launch), timed with CUDA events around its launches."""
+    peak, kind = hbm_peak()
+    cells = nx * ny * nz
+    per_launch = cells * (8.0 * S + 28.0)
+    achieved = per_launch / (total_ms / launches / 1e3) / 1e9 if launches > 0 and total_ms > 0 else None
+    return {
+        "kernel": "k_mpdata_onepass (donor-cell pass, pseudo-velocities, FCT and corrective pass, all species)",
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None, "traffic": cells * S * ONEPASS_DRAM_BYTES_PER_CS,
+        "peak_kind": kind, "algorithmic_bytes_per_launch": per_launch,
+        "launch_ms": (total_ms / launches) if launches else None,
+        "bytes_model": "8 + 28/S B per cell-species; one launch = all species of one advect call",
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per cell-species of a "
+                           "256x256x40x12 launch, scaled to this launch by cell-species"),
     }

@@ -42,6 +42,7 @@ class Request:
     finished: float | None = None
     result: dict | None = None
     footprint: int = 0
+    error: str | None = None       # set when the request failed (it then has no result)
 
     @property
     def cell_species(self) -> int:
@@ -81,16 +82,32 @@ def footprint(req: Request, options: Options) -> int:
     return int(b.value) + 4 * cells * 2 * len(req.species)
 
 
+class InjectedFault(RuntimeError):
+    """A failure raised on the host by the fault hook (tests of the serving loop)."""
+
+
 class Server:
+    """path: MPDATA kernels of the batched step (0 two-pass, 2 single-pass
+    bit-exact, 3 single-pass fast; see icar_adv_set_path).  fault_hook(req,
+    stage, steps_done), if given, is called on the host when a request is set
+    up (stage "setup") and after each of its steps (stage "step"); an
+    exception it raises fails that request alone: the request leaves the
+    batch with its error recorded, and every other request continues."""
+
     def __init__(self, device: int = 0, budget_bytes: float = 150e9, max_slots: int = 512,
-                 options: Options | None = None, keep_results: bool = True, stream=None):
+                 options: Options | None = None, keep_results: bool = True, stream=None, path: int = 0,
+                 fault_hook=None):
         self.device = device
         self.budget = int(budget_bytes)
         self.max_slots = max_slots
         self.options = options or Options()
         self.keep_results = keep_results
+        self.path = path
+        self.fault_hook = fault_hook
+        self.failed: list[Request] = []
         import torch
         self.batch = Batch(device)
+        self.batch.set_path(path)
         # the batch runs on this stream; completion times come from events on it
         self.stream = torch.cuda.Stream(device) if stream is None else torch.cuda.ExternalStream(stream, device)
         self.batch.set_stream(self.stream.cuda_stream)
@@ -124,13 +141,26 @@ class Server:
             if len(self.live) >= self.max_slots or self.used + req.footprint > self.budget:
                 break                      # FIFO: wait for a slot / memory to free up
             self.queue.popleft()
-            fields, dt = device_member(req.nx, req.ny, req.nz, req.seed, device=self.device, species=req.species)
-            dom = Domain.create_on_device(fields, req.nx, req.ny, req.nz, 4000.0, self.options, device=self.device,
-                                          forcing=True)
-            dom._device_fields = None      # the handle holds its own copies now
-            del fields
-            self.batch.add(dom, dt)
             req.admitted = self.now()
+            dom = None
+            try:
+                fields, dt = device_member(req.nx, req.ny, req.nz, req.seed, device=self.device,
+                                           species=req.species)
+                dom = Domain.create_on_device(fields, req.nx, req.ny, req.nz, 4000.0, self.options,
+                                              device=self.device, forcing=True)
+                dom._device_fields = None      # the handle holds its own copies now
+                del fields
+                dom.set_path(self.path)
+                if self.fault_hook is not None:
+                    self.fault_hook(req, "setup", 0)
+                self.batch.add(dom, dt)
+            except Exception as exc:        # this request fails alone; the server carries on
+                if dom is not None:
+                    dom.close()
+                req.error = f"set-up failed: {exc}"
+                req.finished = self.now()
+                self.failed.append(req)
+                continue
             self.used += req.footprint
             self.live.append(_Live(req, dom, req.steps))
             self.peak_used = max(self.peak_used, self.used)
@@ -155,6 +185,17 @@ class Server:
             self._flush_graveyard()
         req.finished = self.now()
         self.done.append(req)
+
+    def _fail(self, lv: _Live, msg: str) -> None:
+        """A request failed between steps: it leaves the batch (no launch of
+        it is in flight once the batch stream has drained past its last
+        step) and its memory is returned; the batch goes on without it."""
+        req = lv.req
+        self.batch.remove(lv.dom)
+        self.graveyard.append((lv.dom, req.footprint))
+        req.error = msg
+        req.finished = self.now()
+        self.failed.append(req)
 
     def _flush_graveyard(self) -> None:
         for dom, fp in self.graveyard:
@@ -190,11 +231,20 @@ class Server:
                 continue
             self.batch.step()
             self.steps += 1
-            finished = []
+            finished, broken = [], []
             for lv in self.live:
                 lv.remaining -= 1
+                if self.fault_hook is not None:
+                    try:
+                        self.fault_hook(lv.req, "step", lv.req.steps - lv.remaining)
+                    except Exception as exc:
+                        broken.append((lv, exc))
+                        continue
                 if lv.remaining == 0:
                     finished.append(lv)
+            for lv, exc in broken:
+                self.live.remove(lv)
+                self._fail(lv, f"failed after {lv.req.steps - lv.remaining} steps: {exc}")
             if finished:
                 ev = torch.cuda.Event(enable_timing=True)
                 ev.record(self.stream)
@@ -220,6 +270,7 @@ class Server:
         work = sum(r.cell_species for r in done)
         return {
             "requests": len(done),
+            "failed": len(self.failed),
             "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)),
             "mean_latency_s": float(lat.mean()),

@@ -10,10 +10,11 @@ from hicar_b200.serve import Request, Server, footprint
 pytestmark = pytest.mark.gpu
 
 
-def alone(req: Request) -> dict:
+def alone(req: Request, path: int = 0) -> dict:
     import torch
     fields, dt = synth.device_member(req.nx, req.ny, req.nz, req.seed, species=req.species)
     d = Domain.create_on_device(fields, req.nx, req.ny, req.nz, 4000.0, Options(), forcing=True)
+    d.set_path(path)
     for _ in range(req.steps):
         step(d, Options(), dt)
     out = {}
@@ -54,4 +55,56 @@ def test_request_over_budget_is_refused():
     srv = Server(budget_bytes=1e6)
     with pytest.raises(ValueError):
         srv.submit(Request(0, 64, 64, 20, 3, 1))
+    srv.close()
+
+
+def test_single_pass_fast_results_are_the_same_alone_and_in_the_mix():
+    """The server on the single-pass fast kernel: a request's result in the
+    mix equals the same request run alone on that kernel (the batched and
+    single-domain launches compute every tile the same way)."""
+    sp = ("qv", "qc", "nr", "theta")
+    reqs = [Request(0, 80, 70, 12, 5, 201, 0.00, sp), Request(1, 130, 60, 9, 7, 202, 0.00, sp),
+            Request(2, 57, 90, 14, 4, 203, 0.03, sp)]
+    srv = Server(path=3)
+    for r in reqs:
+        srv.submit(r)
+    srv.run(max_wall=120)
+    assert srv.report()["requests"] == len(reqs)
+    for r in reqs:
+        ref = alone(r, path=3)
+        for k in sp:
+            assert np.array_equal(r.result[k], ref[k]), (r.rid, k)
+    srv.close()
+
+
+def test_failed_requests_leave_the_batch_and_the_others_are_unaffected():
+    """Failures injected on the host: request 1 fails while it is set up,
+    request 2 after its third step (between steps, none of its work in
+    flight).  Both are reported with their errors and leave the batch; the
+    other requests finish with results identical to running them alone."""
+    from hicar_b200.serve import InjectedFault
+    sp = ("qv", "qc", "nr", "theta")
+    reqs = [Request(0, 48, 40, 10, 6, 301, 0.00, sp), Request(1, 70, 33, 14, 5, 302, 0.00, sp),
+            Request(2, 35, 61, 8, 7, 303, 0.00, sp), Request(3, 64, 52, 11, 8, 304, 0.01, sp)]
+
+    def hook(req, stage, steps_done):
+        if req.rid == 1 and stage == "setup":
+            raise InjectedFault("injected set-up failure")
+        if req.rid == 2 and stage == "step" and steps_done == 3:
+            raise InjectedFault("injected failure between steps")
+
+    srv = Server(fault_hook=hook)
+    for r in reqs:
+        srv.submit(r)
+    srv.run(max_wall=120)
+    rep = srv.report()
+    assert rep["requests"] == 2 and rep["failed"] == 2
+    assert reqs[1].error and "set-up failed" in reqs[1].error and reqs[1].result is None
+    assert reqs[2].error and "after 3 steps" in reqs[2].error and reqs[2].result is None
+    assert not srv.batch.members or all(m is not None for m in srv.batch.members)
+    for r in (reqs[0], reqs[3]):
+        assert r.error is None
+        ref = alone(r)
+        for k in sp:
+            assert np.array_equal(r.result[k], ref[k]), (r.rid, k)
     srv.close()
