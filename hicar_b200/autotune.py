@@ -14,7 +14,8 @@ bit-identical fields; tests/test_autotune_gpu.py checks it):
 
 tune_domain(nx, ny, nz, n_species, fct)
     measures every combination on a synthetic domain of that grid shape,
-    generated on the device, and returns the fastest.  Results are cached per
+    generated on the device, each from the same saved initial state, and
+    returns the fastest.  Results are cached per
     (GPU name, grid shape, species count, FCT) in memory and in a JSON file
     ($HICAR_B200_AUTOTUNE_CACHE, default ~/.cache/hicar_b200/autotune.json).
 shape_costs(fct)
@@ -130,11 +131,37 @@ def _synthetic_domain(nx, ny, nz, n_species, fct, device, seed=12345):
     return dom, opts, dt
 
 
-def _time_advects(dom, opts, dt, shape, group, reps) -> float:
+class _SavedState:
+    """The species of a domain at one moment, kept on the device, so that
+    every candidate is timed from the same state (the cost of a step depends
+    on the fields)."""
+
+    def __init__(self, dom):
+        import torch
+        self.dom = dom
+        self.t = {}
+        for k in dom.adv_vars:
+            t = torch.empty(dom.nx * dom.ny * dom.nz, dtype=torch.float32, device=f"cuda:{dom.device}")
+            dom.fetch_device(k, t)
+            self.t[k] = t
+        dom.sync()
+
+    def restore(self) -> None:
+        import ctypes as C
+        from . import _lib as L
+        lib = L.load()
+        for k, t in self.t.items():
+            L.check(lib.icar_adv_set_field_device(self.dom.handle, L.SPECIES_IDS[k], C.c_void_p(t.data_ptr())),
+                    self.dom.handle)
+
+
+def _time_advects(dom, opts, dt, shape, group, reps, saved: _SavedState | None = None) -> float:
     import ctypes as C
     from . import _lib as L
     from .advection import advect
     lib = L.load()
+    if saved is not None:
+        saved.restore()
     dom.set_launch_shape(shape, group)
     advect(dom, opts, dt)                       # warm-up with this shape
     L.check(lib.icar_adv_profile(dom.handle, 1), dom.handle)
@@ -157,9 +184,10 @@ def tune_domain(nx: int, ny: int, nz: int, n_species: int, fct: bool = True, dev
     dom, opts, dt = _synthetic_domain(nx, ny, nz, n_species, fct, device)
     measured = {}
     try:
+        saved = _SavedState(dom)
         for shape in range(len(TILE_ROWS)):
             for group in species_groups(n_species):
-                measured[f"{shape}:{group}"] = _time_advects(dom, opts, dt, shape, group, reps)
+                measured[f"{shape}:{group}"] = _time_advects(dom, opts, dt, shape, group, reps, saved)
     finally:
         dom.close()
     best = min(measured, key=measured.get)
@@ -183,8 +211,9 @@ def shape_costs(fct: bool = True, device: int = 0, calib=(256, 256, 40, 12), rep
     dom, opts, dt = _synthetic_domain(nx, ny, nz, S, fct, device)
     costs = {}
     try:
+        saved = _SavedState(dom)
         for shape, rows in enumerate(TILE_ROWS):
-            ms = _time_advects(dom, opts, dt, shape, 0, reps)
+            ms = _time_advects(dom, opts, dt, shape, 0, reps, saved)
             costs[shape] = ms / (tiles(nx, ny, rows) * nz * S)
     finally:
         dom.close()
