@@ -5,8 +5,10 @@
 //                 U_m, V_m, W_m (mpdata_compute_wind) plus G = J*rho,
 //                 DJR = dz*J*rho and W' = W_m/dz, formed with exactly the
 //                 reference's operations so every later use is bit-identical.
-//   k_mp_upwind   donor-cell pass q0 -> q1, every species of a cell in one
-//                 thread; also writes the untouched boundary ring of the output.
+//   k_mp_upwind_cols  donor-cell pass q0 -> q1 (upwind_advection,
+//                 adv_mpdata.f90:43-103), one thread per column marching up
+//                 it over staged level planes; also writes the untouched
+//                 boundary ring of the output.
 //   k_mp_corr     antidiffusive pseudo-velocities, FCT limiter and the
 //                 corrective donor-cell pass, fused: one CTA owns a 28x16
 //                 column tile of one species and marches up the column,
@@ -87,70 +89,6 @@ struct SpeciesPtrs {
     float *out[32];
 };
 
-// --------------------------------------------------------------------------
-// donor-cell pass 1 (upwind_advection, adv_mpdata.f90:43-103) for every
-// species of one cell; boundary ring of `out` = q0.  The winds and metric
-// terms of the cell are read once and reused for all its species.
-// --------------------------------------------------------------------------
-__device__ __forceinline__ void mp_upwind_at(const Geo &g, int i, int k, int j, const float *const *q0s,
-                                             float *const *q1s, float *const *outs, int S,
-                                             const float *__restrict__ U, const float *__restrict__ V,
-                                             const float *__restrict__ W, const float *__restrict__ Gc,
-                                             const float *__restrict__ DJR)
-{
-    const size_t c = ix(g, i, k, j);
-    if (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1) {
-        for (int s = 0; s < S; s++) {
-            const float q0 = q0s[s][c];
-            q1s[s][c] = q0;
-            outs[s][c] = q0;
-        }
-        return;
-    }
-    const size_t sy = (size_t)g.P * g.nz, sz = (size_t)g.P;
-    const float ue = U[c + 1], uw = U[c], vn = V[c + sy], vs = V[c];
-    const float wt = W[c], wb = k > 0 ? W[c - sz] : 0.0f;
-    const float G = Gc[c], djr = DJR[c];
-    const bool mid = k > 0 && k < g.nz - 1;
-    for (int s = 0; s < S; s++) {
-        const float *__restrict__ qin = q0s[s];
-        const float q0 = qin[c];
-        const float fe = flux1(q0, qin[c + 1], ue);
-        const float fw = flux1(qin[c - 1], q0, uw);
-        const float f3 = flux1(q0, qin[c + sy], vn);
-        const float f4 = flux1(qin[c - sy], q0, vs);
-        float val = q0 - ((fe - fw) + (f3 - f4)) / G;
-        if (mid) {
-            const float f5t = flux1(q0, qin[c + sz], wt);
-            const float f5b = flux1(qin[c - sz], q0, wb);
-            val = val - (f5t - f5b) / djr;
-        } else if (k == 0) {
-            const float f5t = flux1(q0, qin[c + sz], wt);
-            val = val - f5t / djr;
-        } else {
-            const float f5b = flux1(qin[c - sz], q0, wb);
-            val = val - (q0 * wt - f5b) / djr;
-        }
-        q1s[s][c] = val;
-    }
-}
-
-// Species group: blockIdx.y takes species [y*sg, min(S, (y+1)*sg)) of every
-// cell, so a small domain can trade the reuse of its winds for more blocks.
-__global__ void k_mp_upwind(Geo g, const __grid_constant__ SpeciesPtrs sp, int S, int sg,
-                            const float *__restrict__ U, const float *__restrict__ V, const float *__restrict__ W,
-                            const float *__restrict__ Gc, const float *__restrict__ DJR)
-{
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = (int)(t % (size_t)g.nx);
-    const size_t rest = t / (size_t)g.nx;
-    const int k = (int)(rest % (size_t)g.nz);
-    const int j = (int)(rest / (size_t)g.nz);
-    if (j >= g.ny) return;
-    const int s0 = blockIdx.y * sg;
-    mp_upwind_at(g, i, k, j, sp.q0 + s0, sp.q1 + s0, sp.out + s0, min(sg, S - s0), U, V, W, Gc, DJR);
-}
-
 // Species per group of the donor-cell pass for the knob sg (0 = all species).
 __host__ __device__ inline int upwind_group(int S, int sg) { return sg <= 0 || sg > S ? S : sg; }
 
@@ -198,7 +136,7 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // Donor-cell pass 1 for every species of a species group, one thread per
-// column marching up the column (the same arithmetic as mp_upwind_at, cell
+// column marching up the column (the donor-cell arithmetic of upwind_advection, cell
 // for cell).  CTA tile 32 x 8 columns; blockIdx.z selects the species
 // group.  Each level of every species of the group, and of U_m and V_m,
 // arrives in shared-memory planes by 16-byte cp.async three levels ahead

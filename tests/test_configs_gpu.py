@@ -62,6 +62,36 @@ def test_config2_full_size_100_steps(config2_100):
     print("config 2, 512x512x40, 100 steps: bit-exact vs FP32 oracle; error vs FP64 oracle: " + ", ".join(lines))
 
 
+def test_config2_full_size_100_steps_fast_kernel(config2_100):
+    """The single-pass fast kernel over the same 100 steps.  Its stated
+    tolerance (see tests/test_onepass_fast_gpu.py): every field's error
+    against the FP64 oracle at most 5 times the FP32 oracle's own plus 1e-6,
+    and 99.9 % of the cells within 1e-4 of the FP32 oracle."""
+    case, ref32, ref64 = config2_100
+    opts = Options()
+    d = Domain.from_case(case)
+    adv_init(d, opts)
+    d.use_single_pass(fast=True)
+    for _ in range(100):
+        advect(d, opts, case.dt)
+    out = {k: d.fetch(k).copy() for k in case.species}
+    d.close()
+    lines, bad = [], []
+    for k in case.species:
+        ref = ref32[k].astype(np.float64)
+        scale = max(float(np.abs(ref).max()), 1e-30)
+        r = np.abs(out[k].astype(np.float64) - ref) / np.maximum(np.abs(ref), FLOOR * scale)
+        e_fast, e_ref = rel_err(out[k], ref64[k]), rel_err(ref32[k], ref64[k])
+        p999 = float(np.quantile(r, 0.999))
+        lines.append(f"{k} {e_fast:.2e}/{e_ref:.2e}/{float(r.max()):.2e}/{p999:.1e}")
+        if not (e_fast <= 5 * e_ref + 1e-6 and p999 <= 1e-4):
+            bad.append(k)
+        assert np.isfinite(out[k]).all(), k
+    print("config 2, 512x512x40, 100 steps, fast kernel: error vs FP64 (fast / FP32 oracle), "
+          "max and 99.9th pct vs FP32: " + ", ".join(lines))
+    assert not bad, bad
+
+
 def test_config3_ensemble_full_member_sizes_20_steps(oracle_lib):
     """The first eight members of the config-3 draw the benchmark uses
     (ensemble_shapes(64, 7)), at their full sizes and with all 12 fields,
