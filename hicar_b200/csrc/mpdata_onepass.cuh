@@ -58,10 +58,10 @@ constexpr int S_V = 8;               // V_m, 3 levels
 constexpr int S_WP = 11;             // W_m/dz, 3 levels
 constexpr int S_G = 14;              // J*rho, 3 levels
 // thread-written slots
-constexpr int S_Q1 = 17;             // q1, 4 levels (t-2 .. t+1)
-constexpr int S_V2 = 21;             // unlimited v2 of the current level
-constexpr int S_BYI = 22, S_BYO = 23;  // y-limiter betas of the current level
-constexpr int NPLANES = 24;
+constexpr int S_Q1 = 17;             // q1, 5 levels (t-3 .. t+1)
+constexpr int S_V2 = 22;             // unlimited v2 of the current level
+constexpr int S_BYI = 23, S_BYO = 24;  // y-limiter betas of the current level
+constexpr int NPLANES = 25;
 constexpr size_t SMEM = (size_t)NPLANES * PLANE * sizeof(float) + 128;
 constexpr uint64_t WAIT_NS = 2000000000ull;  // a TMA wait gives up after 2 s
 constexpr int MAXS = 32;             // species per launch
@@ -217,6 +217,26 @@ __device__ __forceinline__ void fct_cell(float q1m, float q1c, float q1p, float 
     bout = beta<EXACT>(q1c - qmin, fout + e15);
 }
 
+// The same terms for a pair of interior cells (pos 0) in the fast
+// variant's packed arithmetic.
+__device__ __forceinline__ void fct_pair_fast(float2 q1m, float2 q1c, float2 q1p, float2 q0m, float2 q0c, float2 q0p,
+                                              float2 fl, float2 fr, float2 &bin, float2 &bout)
+{
+    const float2 qmax = make_float2(fmaxf(fmaxf(fmaxf(q1m.x, q1c.x), q1p.x), fmaxf(fmaxf(q0m.x, q0c.x), q0p.x)),
+                                    fmaxf(fmaxf(fmaxf(q1m.y, q1c.y), q1p.y), fmaxf(fmaxf(q0m.y, q0c.y), q0p.y)));
+    const float2 qmin = make_float2(fminf(fminf(fminf(q1m.x, q1c.x), q1p.x), fminf(fminf(q0m.x, q0c.x), q0p.x)),
+                                    fminf(fminf(fminf(q1m.y, q1c.y), q1p.y), fminf(fminf(q0m.y, q0c.y), q0p.y)));
+    const float2 fin = sub2(make_float2(fmaxf(0.0f, fl.x), fmaxf(0.0f, fl.y)),
+                            make_float2(fminf(0.0f, fr.x), fminf(0.0f, fr.y)));
+    const float2 fout = sub2(make_float2(fmaxf(0.0f, fr.x), fmaxf(0.0f, fr.y)),
+                             make_float2(fminf(0.0f, fl.x), fminf(0.0f, fl.y)));
+    const float2 e15 = splat2(1e-15f);
+    const float2 a = mul2(sub2(qmax, q1c), rcp2(add2(fin, e15)));
+    const float2 b = mul2(sub2(q1c, qmin), rcp2(add2(fout, e15)));
+    bin = make_float2(fminf(1.0f, a.x), fminf(1.0f, a.y));
+    bout = make_float2(fminf(1.0f, b.x), fminf(1.0f, b.y));
+}
+
 // Cross-term ratio (((a-b)+c)-d) / (den + 1e-10) with the reference's
 // operand order for the denominator chosen by the caller.
 __device__ __forceinline__ float2 xnum(float2 a, float2 b, float2 c, float2 d) { return sub2x(add2x(sub2x(a, b), c), d); }
@@ -275,7 +295,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     auto sV = [&](int l) { return P(S_V + l % 3); };
     auto sW = [&](int l) { return P(S_WP + (l + 3) % 3); };   // level -1 maps to a valid slot
     auto sG = [&](int l) { return P(S_G + l % 3); };
-    auto sQ1 = [&](int l) { return P(S_Q1 + ((l + 4) & 3)); };     // levels -2, -1 map to valid slots
+    auto sQ1 = [&](int l) { return P(S_Q1 + (l + 5) % 5); };       // levels -2, -1 map to valid slots
 
     // ---- TMA issue: the loads a level adds (elected thread only)
     // TMA operands must be aligned (map 64 B, destination 128 B, barrier
@@ -311,13 +331,14 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     // the barrier's count at tile start plus the batches issued on it since.
     const uint32_t b0 = ph[0], b1 = ph[1];
     auto phase_of = [&](int t) -> uint32_t { return (t & 1) ? b1 + (uint32_t)(t - 1) / 2 : b0 + (uint32_t)t / 2; };
-    // bounded wait on the batch of iteration t; on a timeout the whole CTA
-    // stops after draining (with a bound) what it issued
-    auto wait_batch = [&](int t) {
-        bool mine = mbar_wait_bounded(&bars[t & 1], phase_of(t) & 1u, WAIT_NS);
-        if (!mine && threadIdx.x == 0) atomicExch(p.err, 1);
-        ok = __syncthreads_and(mine ? 1 : 0) != 0;
-        return ok;
+    // bounded wait on the batch of iteration t, by every thread; a thread
+    // whose wait gave up raises the flag and reports false (the CTA then
+    // agrees at its next barrier to stop, after draining with a bound what
+    // it issued)
+    auto wait_mine = [&](int t) {
+        const bool mine = mbar_wait_bounded(&bars[t & 1], phase_of(t) & 1u, WAIT_NS);
+        if (!mine) atomicExch(p.err, 1);
+        return mine;
     };
     // every batch completes a phase (one arrival, possibly zero bytes): the
     // prologue and the odd iterations on bars[0], the even ones on bars[1]
@@ -362,8 +383,9 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
 
     // own-column values by plain loads, one level ahead
     float2 r_wm[RPW], n_wm[RPW], r_djr0[RPW], r_djrm[RPW], n_djr[RPW], n_dz[RPW];
-    // carried z state of the output cells
-    float2 r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_w2l[RPW], r_part[RPW];
+    // carried z state of the output cells, and the donor pass's flux
+    // through the top of the level it formed last
+    float2 r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_w2l[RPW], r_part[RPW], r_vt[RPW];
     auto ldcol = [&](const float *src, int r, int lev) -> float2 {
         return *reinterpret_cast<const float2 *>(src + rowc[r] + (size_t)lev * lstride);
     };
@@ -375,33 +397,37 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
         n_djr[r] = nz > 1 ? ldcol(p.DJR, r, 1) : splat2(1.0f);
         n_dz[r] = ldcol(p.dz, r, 0);
         r_djrm[r] = splat2(1.0f);
-        r_w2[r] = r_bzi[r] = r_bzo[r] = r_w2l[r] = r_part[r] = splat2(0.0f);
+        r_w2[r] = r_bzi[r] = r_bzo[r] = r_w2l[r] = r_part[r] = r_vt[r] = splat2(0.0f);
     }
 
     const float2 zero2 = splat2(0.0f);
 
     // ---- P0: donor-cell pass at level L into the q1 plane of L ----------
-    // wtop = W_m(L), wbot = W_m(L-1), djr = dz*J*rho at L, own pair.
-    auto donor = [&](int L, int r, float2 wtop, float2 wbot, float2 djr) {
+    // wtop = W_m(L), djr = dz*J*rho at L, own pair.  Levels are formed in
+    // order, so the flux through the bottom of L is the one through the top
+    // of L-1, carried in r_vt.
+    auto donor = [&](int L, int r, float2 wtop, float2 djr) {
         const int Y = rowY[r], j = rowj[r];
         const bool need = Y >= 1 && Y <= PH - 2;     // warp-uniform
         if (!need) return;
         const float *Q = sq0(L);
         const float2 c = ld2(Q, Y, X);
         const float2 n = ld2(Q, Y + 1, X), sth = ld2(Q, Y - 1, X);
-        const float2 w = lft(c), e = rgt(c);
+        const float2 w = lft(c);
         const float2 uw = ld2(sU(L), Y, X);
-        const float2 ue = rgt(uw);
         const float2 vs = ld2(sV(L), Y, X), vn = ld2(sV(L), Y + 1, X);
         const float2 G = ld2(sG(L), Y, X);
-        const float2 fe = flux<EXACT>(c, e, ue), fw = flux<EXACT>(w, c, uw);
+        // a cell's east face is the next cell's west face: same operands,
+        // same value, so it is formed once and passed along by a shuffle
+        const float2 fw = flux<EXACT>(w, c, uw), fe = rgt(fw);
         const float2 f3 = flux<EXACT>(c, n, vn), f4 = flux<EXACT>(sth, c, vs);
         const float2 hd = ad<EXACT>(sb<EXACT>(fe, fw), sb<EXACT>(f3, f4));
         float2 val;
         const bool mid = L > 0 && L < nz - 1;
-        float2 vt = zero2, vb = zero2;
+        float2 vt = zero2;
+        const float2 vb = L > 0 ? r_vt[r] : zero2;
         if (L < nz - 1) vt = flux<EXACT>(c, ld2(sq0(L + 1), Y, X), wtop);
-        if (L > 0) vb = flux<EXACT>(ld2(sq0(L - 1), Y, X), c, wbot);
+        r_vt[r] = vt;
         if constexpr (EXACT) {
             val = sub2x(c, div2x(hd, G));
             if (mid) val = sub2x(val, div2x(sub2x(vt, vb), djr));
@@ -422,23 +448,23 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     };
 
     // ---- prologue: batch 0 landed -> q1 at level 0 ----------------------
-    if (!wait_batch(0)) goto drain;
+    ok = __syncthreads_and(wait_mine(0) ? 1 : 0) != 0;
+    if (!ok) goto drain;
 #pragma unroll
-    for (int r = 0; r < RPW; r++) donor(0, r, r_wm[r], zero2, r_djr0[r]);
-    __syncthreads();
+    for (int r = 0; r < RPW; r++) donor(0, r, r_wm[r], r_djr0[r]);
 
+    // Three block barriers per level: after P0, after P1 (v2 plane), after
+    // P2 (y betas).  P0 of iteration t may overlap P3 of iteration t-1: it
+    // writes the q1 slot of level t+1, which the 5-level ring keeps apart
+    // from the levels t-3 .. t-1 that P3 reads, and reads only TMA planes.
     for (int t = 0; t <= nz; t++) {
-        // everything of iteration t-1 is done: issue the loads iteration t+1 adds
-        if (t > 0) __syncthreads();
-        if (threadIdx.x == 0) issue(&bars[(t + 1) & 1], t + 3, t + 2, t + 2, t + 1, t + 2);
-        if (t >= 1 && !wait_batch(t)) goto drain;
+        const bool landed = t == 0 || wait_mine(t);
 
         const bool haveA = t < nz;
         // own-column values for this iteration; prefetch the next level's
-        float2 c_wm[RPW], c_wmn[RPW], c_djrn[RPW], c_dz[RPW];
+        float2 c_wmn[RPW], c_djrn[RPW], c_dz[RPW];
 #pragma unroll
         for (int r = 0; r < RPW; r++) {
-            c_wm[r] = r_wm[r];
             c_wmn[r] = n_wm[r];
             c_djrn[r] = n_djr[r];
             c_dz[r] = n_dz[r];
@@ -452,9 +478,16 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
         // ---- P0: q1 at level t+1 ------------------------------------------
         if (t + 1 < nz) {
 #pragma unroll
-            for (int r = 0; r < RPW; r++) donor(t + 1, r, c_wmn[r], c_wm[r], c_djrn[r]);
+            for (int r = 0; r < RPW; r++) donor(t + 1, r, c_wmn[r], c_djrn[r]);
         }
-        __syncthreads();
+        // every thread is past iteration t-1 and the batch of iteration t
+        // landed (or the CTA stops): the planes that batch t+1 overwrites
+        // (q0 of t-2, U_m, V_m, J*rho of t-1, W_m/dz of t-2) are free.  The
+        // elected thread's warp has one row with nothing to do in P1, so
+        // the issue costs no time on the block's critical path.
+        ok = __syncthreads_and(landed ? 1 : 0) != 0;
+        if (!ok) goto drain;
+        if (threadIdx.x == 0) issue(&bars[(t + 1) & 1], t + 3, t + 2, t + 2, t + 1, t + 2);
 
         float2 u2[RPW], v2[RPW], w2[RPW], fz[RPW];
         float2 bxi[RPW], bxo[RPW], byi[RPW], byo[RPW], bzi[RPW], bzo[RPW];
@@ -649,12 +682,17 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                 const float2 qcl = lft(qc), qcr = rgt(qc), q0l = lft(q0c), q0r = rgt(q0c);
                 // x lines: faces ia, ib, ib+1
                 {
-                    const float2 ur = rgt(u2[r]);
-                    const float2 fl = flux<EXACT>(qcl, qc, u2[r]), fr = flux<EXACT>(qc, qcr, ur);
-                    const int pa = INT ? 0 : (ia == 0 ? 1 : (ia == nx - 1 ? 2 : 0));
-                    const int pb = INT ? 0 : (ib == 0 ? 1 : (ib == nx - 1 ? 2 : 0));
-                    fct_cell<EXACT>(qcl.x, qc.x, qcr.x, q0l.x, q0c.x, q0r.x, fl.x, fr.x, pa, false, bxi[r].x, bxo[r].x);
-                    fct_cell<EXACT>(qcl.y, qc.y, qcr.y, q0l.y, q0c.y, q0r.y, fl.y, fr.y, pb, false, bxi[r].y, bxo[r].y);
+                    const float2 fl = flux<EXACT>(qcl, qc, u2[r]), fr = rgt(fl);
+                    if constexpr (INT && !EXACT) {
+                        fct_pair_fast(qcl, qc, qcr, q0l, q0c, q0r, fl, fr, bxi[r], bxo[r]);
+                    } else {
+                        const int pa = INT ? 0 : (ia == 0 ? 1 : (ia == nx - 1 ? 2 : 0));
+                        const int pb = INT ? 0 : (ib == 0 ? 1 : (ib == nx - 1 ? 2 : 0));
+                        fct_cell<EXACT>(qcl.x, qc.x, qcr.x, q0l.x, q0c.x, q0r.x, fl.x, fr.x, pa, false, bxi[r].x,
+                                        bxo[r].x);
+                        fct_cell<EXACT>(qcl.y, qc.y, qcr.y, q0l.y, q0c.y, q0r.y, fl.y, fr.y, pb, false, bxi[r].y,
+                                        bxo[r].y);
+                    }
                 }
                 // y lines: faces j and j+1
                 {
@@ -662,9 +700,15 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     const float2 q0n = ld2(sq0(t), Y + 1, X), q0s = ld2(sq0(t), Y - 1, X);
                     const float2 vn = ld2(P(S_V2), Y + 1, X);
                     const float2 fl = flux<EXACT>(qs, qc, v2[r]), fr = flux<EXACT>(qc, qn, vn);
-                    const int pj = INT ? 0 : (j == 0 ? 1 : (j == ny - 1 ? 2 : 0));
-                    fct_cell<EXACT>(qs.x, qc.x, qn.x, q0s.x, q0c.x, q0n.x, fl.x, fr.x, pj, false, byi[r].x, byo[r].x);
-                    fct_cell<EXACT>(qs.y, qc.y, qn.y, q0s.y, q0c.y, q0n.y, fl.y, fr.y, pj, false, byi[r].y, byo[r].y);
+                    if constexpr (INT && !EXACT) {
+                        fct_pair_fast(qs, qc, qn, q0s, q0c, q0n, fl, fr, byi[r], byo[r]);
+                    } else {
+                        const int pj = INT ? 0 : (j == 0 ? 1 : (j == ny - 1 ? 2 : 0));
+                        fct_cell<EXACT>(qs.x, qc.x, qn.x, q0s.x, q0c.x, q0n.x, fl.x, fr.x, pj, false, byi[r].x,
+                                        byo[r].x);
+                        fct_cell<EXACT>(qs.y, qc.y, qn.y, q0s.y, q0c.y, q0n.y, fl.y, fr.y, pj, false, byi[r].y,
+                                        byo[r].y);
+                    }
                     st2(P(S_BYI), Y, X, byi[r]);
                     st2(P(S_BYO), Y, X, byo[r]);
                 }
@@ -677,10 +721,14 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     // flux through the top of level t-1, as P1 formed it one level ago
                     const float2 fzd = flux<EXACT>(qd, qc, r_w2[r]);
                     const int pz = t == 0 ? 1 : (t == nz - 1 ? 2 : 0);
-                    fct_cell<EXACT>(qd.x, qc.x, qu.x, q0d.x, q0c.x, q0u.x, fzd.x, fz[r].x, pz, true, bzi[r].x,
-                                    bzo[r].x);
-                    fct_cell<EXACT>(qd.y, qc.y, qu.y, q0d.y, q0c.y, q0u.y, fzd.y, fz[r].y, pz, true, bzi[r].y,
-                                    bzo[r].y);
+                    if (!EXACT && pz == 0) {
+                        fct_pair_fast(qd, qc, qu, q0d, q0c, q0u, fzd, fz[r], bzi[r], bzo[r]);
+                    } else {
+                        fct_cell<EXACT>(qd.x, qc.x, qu.x, q0d.x, q0c.x, q0u.x, fzd.x, fz[r].x, pz, true, bzi[r].x,
+                                        bzo[r].x);
+                        fct_cell<EXACT>(qd.y, qc.y, qu.y, q0d.y, q0c.y, q0u.y, fzd.y, fz[r].y, pz, true, bzi[r].y,
+                                        bzo[r].y);
+                    }
                 }
             }
             __syncthreads();   // y betas complete
@@ -694,16 +742,13 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
             float2 n_part = zero2, n_w2l = zero2;
             if (haveA && outrow) {
                 const float2 qc = ld2(sQ1(t), Y, X), qn = ld2(sQ1(t), Y + 1, X), qs = ld2(sQ1(t), Y - 1, X);
-                const float2 qcl = lft(qc), qcr = rgt(qc);
+                const float2 qcl = lft(qc);
                 float2 uw = u2[r];
-                float2 ue = rgt(u2[r]);
                 float2 vs = v2[r], vn = ld2(P(S_V2), Y + 1, X);
                 if (FCT) {
-                    const float2 bil = lft(bxi[r]), bol = lft(bxo[r]), bir = rgt(bxi[r]), bor = rgt(bxo[r]);
+                    const float2 bil = lft(bxi[r]), bol = lft(bxo[r]);
                     uw.x = limit<EXACT>(uw.x, bxi[r].x, bol.x, bil.x, bxo[r].x);
                     uw.y = limit<EXACT>(uw.y, bxi[r].y, bxo[r].x, bxi[r].x, bxo[r].y);
-                    ue.x = uw.y;
-                    ue.y = limit<EXACT>(ue.y, bir.y, bxo[r].y, bxi[r].y, bor.y);
                     const float2 bis = ld2(P(S_BYI), Y - 1, X), bos = ld2(P(S_BYO), Y - 1, X);
                     const float2 bin = ld2(P(S_BYI), Y + 1, X), bon = ld2(P(S_BYO), Y + 1, X);
                     vs.x = limit<EXACT>(vs.x, byi[r].x, bos.x, bis.x, byo[r].x);
@@ -711,7 +756,8 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     vn.x = limit<EXACT>(vn.x, bin.x, byo[r].x, byi[r].x, bon.x);
                     vn.y = limit<EXACT>(vn.y, bin.y, byo[r].y, byi[r].y, bon.y);
                 }
-                const float2 fe = flux<EXACT>(qc, qcr, ue), fw = flux<EXACT>(qcl, qc, uw);
+                // east faces as the next cell's limited west faces
+                const float2 fw = flux<EXACT>(qcl, qc, uw), fe = rgt(fw);
                 const float2 f3 = flux<EXACT>(qc, qn, vn), f4 = flux<EXACT>(qs, qc, vs);
                 const float2 hd = ad<EXACT>(sb<EXACT>(fe, fw), sb<EXACT>(f3, f4));
                 const float2 G = ld2(sG(t), Y, X);
@@ -777,7 +823,6 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
             }
             r_djrm[r] = r_djr0[r];
             r_djr0[r] = c_djrn[r];
-            r_wm[r] = c_wmn[r];
         }
     }
     return true;
