@@ -176,6 +176,20 @@ __device__ __forceinline__ float limit(float u, float bin_r, float bout_l, float
     }
 }
 
+// Limited flux through a pair of faces in the fast variant: the face
+// velocity u times the limiter factor of its sign (min(bin_r, bout_l) for
+// u > 0, min(bin_l, bout_r) otherwise) times the upwind cell's value; one
+// comparison per face serves both selects.
+__device__ __forceinline__ float2 lim_flux2(float2 u, float2 ql, float2 qr, float2 bin_r, float2 bout_l, float2 bin_l,
+                                            float2 bout_r)
+{
+    const bool px = u.x > 0.0f, py = u.y > 0.0f;
+    const float2 b = make_float2(fminf(px ? bin_r.x : bin_l.x, px ? bout_l.x : bout_r.x),
+                                 fminf(py ? bin_r.y : bin_l.y, py ? bout_l.y : bout_r.y));
+    const float2 q = make_float2(px ? ql.x : qr.x, py ? ql.y : qr.y);
+    return mul2(mul2(u, b), q);
+}
+
 // Per-cell limiter terms of one direction (the carried form of the FCT
 // sweep): bounds over the cell and its two line neighbours, in/out flux sums
 // from the fluxes on its two faces, with the reference's first/last-cell
@@ -385,7 +399,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     float2 r_wm[RPW], n_wm[RPW], r_djr0[RPW], r_djrm[RPW], n_djr[RPW], n_dz[RPW];
     // carried z state of the output cells, and the donor pass's flux
     // through the top of the level it formed last
-    float2 r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_w2l[RPW], r_part[RPW], r_vt[RPW];
+    float2 r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_fb[RPW], r_part[RPW], r_vt[RPW];
     auto ldcol = [&](const float *src, int r, int lev) -> float2 {
         return *reinterpret_cast<const float2 *>(src + rowc[r] + (size_t)lev * lstride);
     };
@@ -397,7 +411,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
         n_djr[r] = nz > 1 ? ldcol(p.DJR, r, 1) : splat2(1.0f);
         n_dz[r] = ldcol(p.dz, r, 0);
         r_djrm[r] = splat2(1.0f);
-        r_w2[r] = r_bzi[r] = r_bzo[r] = r_w2l[r] = r_part[r] = r_vt[r] = splat2(0.0f);
+        r_w2[r] = r_bzi[r] = r_bzo[r] = r_fb[r] = r_part[r] = r_vt[r] = splat2(0.0f);
     }
 
     const float2 zero2 = splat2(0.0f);
@@ -530,28 +544,25 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                         }
                         val = mul2x(val, splat2(0.5f));
                     } else {
-                        const float2 rG = rcp2(Gs), a = abs2(Ut);
-                        // 0.5 |U| (1 - 2 |U| / Gs)
-                        const float2 F0 = mul2(mul2(splat2(0.5f), a), fma2(make_float2(-2.0f * a.x, -2.0f * a.y), rG,
-                                                                           splat2(1.0f)));
-                        const float2 S = add2(qc, qcl), D = sub2(qc, qcl);
-                        val = mul2(mul2(F0, D), rcp2(add2(S, splat2(1e-10f))));
-                        const float2 cu = mul2(mul2(splat2(0.25f), Ut), rG);
+                        // the final 0.5 folded in: 0.5 |U| (1 - 2 |U| / Gs) = 0.5 |U| - U^2 / Gs, and each
+                        // cross term 0.25 U / Gs times the 4-face average (1/4 of the face sum) times eq
+                        const float2 rG = rcp2(Gs);
+                        const float2 F0 = sub2(mul2(splat2(0.5f), abs2(Ut)), mul2(mul2(Ut, Ut), rG));
+                        val = mul2(mul2(F0, sub2(qc, qcl)), rcp2(add2(add2(qc, qcl), splat2(1e-10f))));
+                        const float2 mc = mul2(splat2(-0.0625f), mul2(Ut, rG));
                         if (jint) {
                             const float2 qn = ld2(Qc, Y + 1, X), qs = ld2(Qc, Y - 1, X);
-                            const float2 Vt = ld2(Vc, Y, X), Vtn = ld2(Vc, Y + 1, X);
+                            const float2 sv = add2(ld2(Vc, Y, X), ld2(Vc, Y + 1, X));
                             const float2 xp = add2(qn, lft(qn)), xm = add2(qs, lft(qs));
                             const float2 eq = mul2(sub2(xp, xm), rcp2(add2(add2(xp, xm), splat2(1e-10f))));
-                            const float2 ev = mul2(splat2(0.25f), add2(add2(Vt, Vtn), add2(lft(Vt), lft(Vtn))));
-                            val = fma2(make_float2(-cu.x * ev.x, -cu.y * ev.y), eq, val);
+                            val = fma2(mul2(mc, add2(sv, lft(sv))), eq, val);
                         }
                         if (kint) {
                             const float2 qu = ld2(Qu, Y, X), qd = ld2(Qd, Y, X);
-                            const float2 Wt = ld2(Wc, Y, X), Wd = ld2(Wdn, Y, X);
+                            const float2 sw = add2(ld2(Wc, Y, X), ld2(Wdn, Y, X));
                             const float2 xp = add2(qu, lft(qu)), xm = add2(qd, lft(qd));
                             const float2 eq = mul2(sub2(xp, xm), rcp2(add2(add2(xp, xm), splat2(1e-10f))));
-                            const float2 ev = mul2(splat2(0.25f), add2(add2(Wt, Wd), add2(lft(Wt), lft(Wd))));
-                            val = fma2(make_float2(-cu.x * ev.x, -cu.y * ev.y), eq, val);
+                            val = fma2(mul2(mc, add2(sw, lft(sw))), eq, val);
                         }
                     }
                     u2[r] = val;
@@ -565,11 +576,11 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     const float2 qc = ld2(Qc, Y, X), qs = ld2(Qc, Y - 1, X);
                     const float2 Vt = ld2(Vc, Y, X), Gs = ad<EXACT>(ld2(Gcp, Y, X), ld2(Gcp, Y - 1, X));
                     const float2 Ut = ld2(Uc, Y, X), Us = ld2(Uc, Y - 1, X);
-                    const float2 qcl = lft(qc), qcr = rgt(qc), qsl = lft(qs), qsr = rgt(qs);
-                    const float2 Utr = rgt(Ut), Usr = rgt(Us);
                     const bool xa = INT || (ia > 0 && ia < nx - 1), xb = INT || (ib > 0 && ib < nx - 1);
                     float2 val;
                     if constexpr (EXACT) {
+                        const float2 qcl = lft(qc), qcr = rgt(qc), qsl = lft(qs), qsr = rgt(qs);
+                        const float2 Utr = rgt(Ut), Usr = rgt(Us);
                         val = base_x(Vt, Gs, qc, qs);
                         float2 eq = div2x(xnum(make_float2(qs.y, qsr.y), qcl, make_float2(qc.y, qcr.y), qsl),
                                           xden(make_float2(qc.y, qcr.y), make_float2(qs.y, qsr.y), qcl, qsl));
@@ -587,30 +598,26 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                         }
                         val = mul2x(val, splat2(0.5f));
                     } else {
-                        const float2 rG = rcp2(Gs), a = abs2(Vt);
-                        const float2 F0 = mul2(mul2(splat2(0.5f), a), fma2(make_float2(-2.0f * a.x, -2.0f * a.y), rG,
-                                                                           splat2(1.0f)));
-                        const float2 S = add2(qc, qs), D = sub2(qc, qs);
-                        val = mul2(mul2(F0, D), rcp2(add2(S, splat2(1e-10f))));
-                        const float2 cv = mul2(mul2(splat2(0.25f), Vt), rG);
-                        // VxU: pair sums of the two rows at x+1 and x-1
-                        const float2 yp = add2(make_float2(qc.y, qcr.y), make_float2(qs.y, qsr.y));
-                        const float2 ym = add2(qcl, qsl);
+                        const float2 rG = rcp2(Gs);
+                        const float2 F0 = sub2(mul2(splat2(0.5f), abs2(Vt)), mul2(mul2(Vt, Vt), rG));
+                        val = mul2(mul2(F0, sub2(qc, qs)), rcp2(add2(add2(qc, qs), splat2(1e-10f))));
+                        const float2 mc = mul2(splat2(-0.0625f), mul2(Vt, rG));
+                        // x cross term: the two rows' pair sums at x+1 and x-1, and U_m on the
+                        // cells' west and east faces in both rows, each formed from one shuffle
+                        const float2 sq = add2(qc, qs), yp = rgt(sq), ym = lft(sq);
                         const float2 eq = mul2(sub2(yp, ym), rcp2(add2(add2(yp, ym), splat2(1e-10f))));
-                        float2 ev = mul2(splat2(0.25f), add2(add2(make_float2(Ut.y, Utr.y), make_float2(Us.y, Usr.y)),
-                                                             add2(Ut, Us)));
+                        const float2 su = add2(Ut, Us);
+                        float2 ev = add2(su, rgt(su));
                         if (!xa) ev.x = 0.0f;
                         if (!xb) ev.y = 0.0f;
-                        val = fma2(make_float2(-cv.x * ev.x, -cv.y * ev.y), eq, val);
+                        val = fma2(mul2(mc, ev), eq, val);
                         if (kint) {
-                            const float2 qu = ld2(Qu, Y, X), qd = ld2(Qd, Y, X);
-                            const float2 qsu = ld2(Qu, Y - 1, X), qsd = ld2(Qd, Y - 1, X);
-                            const float2 Wt = ld2(Wc, Y, X), Wd = ld2(Wdn, Y, X);
-                            const float2 Wts = ld2(Wc, Y - 1, X), Wds = ld2(Wdn, Y - 1, X);
-                            const float2 zp = add2(qu, qsu), zm = add2(qd, qsd);
+                            const float2 zp = add2(ld2(Qu, Y, X), ld2(Qu, Y - 1, X));
+                            const float2 zm = add2(ld2(Qd, Y, X), ld2(Qd, Y - 1, X));
                             const float2 eq2 = mul2(sub2(zp, zm), rcp2(add2(add2(zp, zm), splat2(1e-10f))));
-                            const float2 ev2 = mul2(splat2(0.25f), add2(add2(Wt, Wd), add2(Wts, Wds)));
-                            val = fma2(make_float2(-cv.x * ev2.x, -cv.y * ev2.y), eq2, val);
+                            const float2 sw = add2(add2(ld2(Wc, Y, X), ld2(Wdn, Y, X)),
+                                                   add2(ld2(Wc, Y - 1, X), ld2(Wdn, Y - 1, X)));
+                            val = fma2(mul2(mc, sw), eq2, val);
                         }
                     }
                     v2[r] = val;
@@ -630,10 +637,10 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     const float2 qnu = ld2(Qu, Y + 1, X), qsu = ld2(Qu, Y - 1, X);
                     const float2 Vt = ld2(Vc, Y, X), Vtn = ld2(Vc, Y + 1, X);
                     const float2 Vu = ld2(Vup, Y, X), Vun = ld2(Vup, Y + 1, X);
-                    const float2 qcl = lft(qc), qcr = rgt(qc), qul = lft(qu), qur = rgt(qu);
-                    const float2 Utr = rgt(Ut), Uur = rgt(Uu);
                     float2 val;
                     if constexpr (EXACT) {
+                        const float2 qcl = lft(qc), qcr = rgt(qc), qul = lft(qu), qur = rgt(qu);
+                        const float2 Utr = rgt(Ut), Uur = rgt(Uu);
                         val = base_x(Wt, Gs, qu, qc);
                         val = cross_x(val, Wt, avg4(make_float2(Ut.y, Utr.y), make_float2(Uu.y, Uur.y), Ut, Uu),
                                       div2x(xnum(make_float2(qu.y, qur.y), qcl, make_float2(qc.y, qcr.y), qul),
@@ -643,22 +650,18 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                                       Gs);
                         val = mul2x(mul2x(val, splat2(0.5f)), c_dz[r]);
                     } else {
-                        const float2 rG = rcp2(Gs), a = abs2(Wt);
-                        const float2 F0 = mul2(mul2(splat2(0.5f), a), fma2(make_float2(-2.0f * a.x, -2.0f * a.y), rG,
-                                                                           splat2(1.0f)));
-                        const float2 S = add2(qu, qc), D = sub2(qu, qc);
-                        val = mul2(mul2(F0, D), rcp2(add2(S, splat2(1e-10f))));
-                        const float2 cw = mul2(mul2(splat2(0.25f), Wt), rG);
-                        const float2 zp = add2(make_float2(qc.y, qcr.y), make_float2(qu.y, qur.y));
-                        const float2 zm = add2(qcl, qul);
+                        const float2 rG = rcp2(Gs);
+                        const float2 F0 = sub2(mul2(splat2(0.5f), abs2(Wt)), mul2(mul2(Wt, Wt), rG));
+                        val = mul2(mul2(F0, sub2(qu, qc)), rcp2(add2(add2(qu, qc), splat2(1e-10f))));
+                        const float2 mc = mul2(splat2(-0.0625f), mul2(Wt, rG));
+                        const float2 sq = add2(qc, qu), zp = rgt(sq), zm = lft(sq);
                         const float2 eq = mul2(sub2(zp, zm), rcp2(add2(add2(zp, zm), splat2(1e-10f))));
-                        const float2 ev = mul2(splat2(0.25f), add2(add2(make_float2(Ut.y, Utr.y), make_float2(Uu.y, Uur.y)),
-                                                                   add2(Ut, Uu)));
-                        val = fma2(make_float2(-cw.x * ev.x, -cw.y * ev.y), eq, val);
+                        const float2 su = add2(Ut, Uu);
+                        val = fma2(mul2(mc, add2(su, rgt(su))), eq, val);
                         const float2 np = add2(qn, qnu), sp = add2(qs, qsu);
                         const float2 eq2 = mul2(sub2(np, sp), rcp2(add2(add2(np, sp), splat2(1e-10f))));
-                        const float2 ev2 = mul2(splat2(0.25f), add2(add2(Vt, Vu), add2(Vtn, Vun)));
-                        val = fma2(make_float2(-cw.x * ev2.x, -cw.y * ev2.y), eq2, val);
+                        const float2 sv = add2(add2(Vt, Vu), add2(Vtn, Vun));
+                        val = fma2(mul2(mc, sv), eq2, val);
                         val = mul2(val, c_dz[r]);
                     }
                     w2[r] = val;
@@ -739,60 +742,83 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
         for (int r = 0; r < RPW; r++) {
             const int Y = rowY[r], j = rowj[r];
             const bool outrow = Y >= 3 && Y <= PH - 4;      // warp-uniform
-            float2 n_part = zero2, n_w2l = zero2;
+            // n_ft: the limited flux through the top of level t-1, formed with
+            // the level-t betas and carried to the next level as its bottom flux
+            float2 n_part = zero2, n_ft = zero2;
             if (haveA && outrow) {
                 const float2 qc = ld2(sQ1(t), Y, X), qn = ld2(sQ1(t), Y + 1, X), qs = ld2(sQ1(t), Y - 1, X);
                 const float2 qcl = lft(qc);
-                float2 uw = u2[r];
-                float2 vs = v2[r], vn = ld2(P(S_V2), Y + 1, X);
-                if (FCT) {
-                    const float2 bil = lft(bxi[r]), bol = lft(bxo[r]);
-                    uw.x = limit<EXACT>(uw.x, bxi[r].x, bol.x, bil.x, bxo[r].x);
-                    uw.y = limit<EXACT>(uw.y, bxi[r].y, bxo[r].x, bxi[r].x, bxo[r].y);
+                const float2 vn0 = ld2(P(S_V2), Y + 1, X);
+                float2 fw, f3, f4;
+                if constexpr (EXACT) {
+                    float2 uw = u2[r], vs = v2[r], vn = vn0;
+                    if (FCT) {
+                        const float2 bil = lft(bxi[r]), bol = lft(bxo[r]);
+                        uw.x = limit<EXACT>(uw.x, bxi[r].x, bol.x, bil.x, bxo[r].x);
+                        uw.y = limit<EXACT>(uw.y, bxi[r].y, bxo[r].x, bxi[r].x, bxo[r].y);
+                        const float2 bis = ld2(P(S_BYI), Y - 1, X), bos = ld2(P(S_BYO), Y - 1, X);
+                        const float2 bin = ld2(P(S_BYI), Y + 1, X), bon = ld2(P(S_BYO), Y + 1, X);
+                        vs.x = limit<EXACT>(vs.x, byi[r].x, bos.x, bis.x, byo[r].x);
+                        vs.y = limit<EXACT>(vs.y, byi[r].y, bos.y, bis.y, byo[r].y);
+                        vn.x = limit<EXACT>(vn.x, bin.x, byo[r].x, byi[r].x, bon.x);
+                        vn.y = limit<EXACT>(vn.y, bin.y, byo[r].y, byi[r].y, bon.y);
+                    }
+                    fw = flux_x(qcl, qc, uw);
+                    f3 = flux_x(qc, qn, vn);
+                    f4 = flux_x(qs, qc, vs);
+                } else if (FCT) {
                     const float2 bis = ld2(P(S_BYI), Y - 1, X), bos = ld2(P(S_BYO), Y - 1, X);
                     const float2 bin = ld2(P(S_BYI), Y + 1, X), bon = ld2(P(S_BYO), Y + 1, X);
-                    vs.x = limit<EXACT>(vs.x, byi[r].x, bos.x, bis.x, byo[r].x);
-                    vs.y = limit<EXACT>(vs.y, byi[r].y, bos.y, bis.y, byo[r].y);
-                    vn.x = limit<EXACT>(vn.x, bin.x, byo[r].x, byi[r].x, bon.x);
-                    vn.y = limit<EXACT>(vn.y, bin.y, byo[r].y, byi[r].y, bon.y);
+                    fw = lim_flux2(u2[r], qcl, qc, bxi[r], lft(bxo[r]), lft(bxi[r]), bxo[r]);
+                    f4 = lim_flux2(v2[r], qs, qc, byi[r], bos, bis, byo[r]);
+                    f3 = lim_flux2(vn0, qc, qn, bin, byo[r], byi[r], bon);
+                } else {
+                    fw = flux_f(qcl, qc, u2[r]);
+                    f3 = flux_f(qc, qn, vn0);
+                    f4 = flux_f(qs, qc, v2[r]);
                 }
                 // east faces as the next cell's limited west faces
-                const float2 fw = flux<EXACT>(qcl, qc, uw), fe = rgt(fw);
-                const float2 f3 = flux<EXACT>(qc, qn, vn), f4 = flux<EXACT>(qs, qc, vs);
+                const float2 fe = rgt(fw);
                 const float2 hd = ad<EXACT>(sb<EXACT>(fe, fw), sb<EXACT>(f3, f4));
                 const float2 G = ld2(sG(t), Y, X);
                 if constexpr (EXACT) n_part = sub2x(qc, div2x(hd, G));
                 else n_part = fma2(make_float2(-hd.x, -hd.y), rcp2(G), qc);
-                // limited w2 at the top of level t-1
-                float2 w = r_w2[r];
-                if (FCT && t >= 1) {
-                    w.x = limit<EXACT>(w.x, bzi[r].x, r_bzo[r].x, r_bzi[r].x, bzo[r].x);
-                    w.y = limit<EXACT>(w.y, bzi[r].y, r_bzo[r].y, r_bzi[r].y, bzo[r].y);
+                if (t >= 1) {
+                    const float2 qd = ld2(sQ1(t - 1), Y, X);
+                    if constexpr (EXACT) {
+                        float2 w = r_w2[r];
+                        if (FCT) {
+                            w.x = limit<EXACT>(w.x, bzi[r].x, r_bzo[r].x, r_bzi[r].x, bzo[r].x);
+                            w.y = limit<EXACT>(w.y, bzi[r].y, r_bzo[r].y, r_bzi[r].y, bzo[r].y);
+                        }
+                        n_ft = flux_x(qd, qc, w);
+                    } else if (FCT) {
+                        n_ft = lim_flux2(r_w2[r], qd, qc, bzi[r], r_bzo[r], r_bzi[r], bzo[r]);
+                    } else {
+                        n_ft = flux_f(qd, qc, r_w2[r]);
+                    }
                 }
-                n_w2l = w;
             }
             // vertical part of level L = t-1 and the store
             if (t >= 1 && outrow) {
                 const int L = t - 1;
-                const float2 qc = ld2(sQ1(L), Y, X);
-                const float2 qa = haveA ? ld2(sQ1(t), Y, X) : zero2;
-                const float2 qdd = L > 0 ? ld2(sQ1(L - 1), Y, X) : zero2;
-                const float2 wtop = n_w2l, wbot = r_w2l[r];
                 float2 val = r_part[r];
                 const float2 djr = r_djrm[r];
                 if constexpr (EXACT) {
                     if (L > 0 && L < nz - 1) {
-                        val = sub2x(val, div2x(sub2x(flux_x(qc, qa, wtop), flux_x(qdd, qc, wbot)), djr));
+                        val = sub2x(val, div2x(sub2x(n_ft, r_fb[r]), djr));
                     } else if (L == 0) {
-                        val = sub2x(val, div2x(flux_x(qc, qa, wtop), djr));
+                        val = sub2x(val, div2x(n_ft, djr));
                     } else {
-                        val = sub2x(val, div2x(sub2x(mul2x(qc, wtop), flux_x(qdd, qc, wbot)), djr));
+                        // the model top: q times the (zero) face velocity there
+                        const float2 qc = ld2(sQ1(L), Y, X);
+                        val = sub2x(val, div2x(sub2x(mul2x(qc, zero2), r_fb[r]), djr));
                     }
                 } else {
                     float2 vd;
-                    if (L > 0 && L < nz - 1) vd = sub2(flux_f(qc, qa, wtop), flux_f(qdd, qc, wbot));
-                    else if (L == 0) vd = flux_f(qc, qa, wtop);
-                    else vd = sub2(mul2(qc, wtop), flux_f(qdd, qc, wbot));
+                    if (L > 0 && L < nz - 1) vd = sub2(n_ft, r_fb[r]);
+                    else if (L == 0) vd = n_ft;
+                    else vd = make_float2(-r_fb[r].x, -r_fb[r].y);   // nothing leaves through the model top
                     val = fma2(make_float2(-vd.x, -vd.y), rcp2(djr), val);
                 }
                 const bool jin = INT || (j >= 0 && j < ny);
@@ -815,7 +841,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
             }
             // rotate the carried state
             if (haveA) {
-                r_w2l[r] = n_w2l;
+                r_fb[r] = n_ft;
                 r_part[r] = n_part;
                 r_w2[r] = w2[r];
                 r_bzi[r] = bzi[r];
