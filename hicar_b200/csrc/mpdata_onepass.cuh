@@ -100,10 +100,16 @@ __device__ __forceinline__ float dn(float v) { return __shfl_down_sync(FULL, v, 
 __device__ __forceinline__ float2 lft(float2 v) { return make_float2(up(v.y), v.x); }
 __device__ __forceinline__ float2 rgt(float2 v) { return make_float2(v.y, dn(v.x)); }
 
+// Hardware reciprocal approximation, flushing subnormal operands and results.
+// Every divisor of the fast variant is a metric term (J*rho, dz*J*rho and
+// their face sums), a sum of tracer values plus 1e-10, or a flux sum plus
+// 1e-15: none is subnormal or above 2^126, so flushing changes no result,
+// and it spares the multi-instruction subnormal handling around each
+// reciprocal that the non-flushing form needs.
 __device__ __forceinline__ float rcp_approx(float x)
 {
     float r;
-    asm("rcp.approx.f32 %0, %1;\n" : "=f"(r) : "f"(x));
+    asm("rcp.approx.ftz.f32 %0, %1;\n" : "=f"(r) : "f"(x));
     return r;
 }
 __device__ __forceinline__ float2 rcp2(float2 b) { return make_float2(rcp_approx(b.x), rcp_approx(b.y)); }
