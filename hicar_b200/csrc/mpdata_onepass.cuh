@@ -257,6 +257,27 @@ __device__ __forceinline__ void fct_pair_fast(float2 q1m, float2 q1c, float2 q1p
     bout = make_float2(fminf(1.0f, b.x), fminf(1.0f, b.y));
 }
 
+// The first and last cells of an x or y line in the fast variant, as the
+// interior form on substituted operands: a neighbour the reference's bounds
+// leave out takes a value already in them (the first cell's bounds omit the
+// cell before it; the last cell's take q1 of the cell before it and of
+// itself and q0 of the cell before it only), and both fluxes are zero (the
+// x and y lines carry no flux sums at their ends).
+__device__ __forceinline__ void fct_edge_sub(bool first, bool last, float &q1m, float q1c, float &q1p, float &q0m,
+                                             float &q0c, float &q0p, float &fl, float &fr)
+{
+    if (first) {
+        q1m = q1c;
+        q0m = q0c;
+    }
+    if (last) {
+        q1p = q1c;
+        q0c = q0m;
+        q0p = q0m;
+    }
+    if (first || last) fl = fr = 0.0f;
+}
+
 // Cross-term ratio (((a-b)+c)-d) / (den + 1e-10) with the reference's
 // operand order for the denominator chosen by the caller.
 __device__ __forceinline__ float2 xnum(float2 a, float2 b, float2 c, float2 d) { return sub2x(add2x(sub2x(a, b), c), d); }
@@ -303,7 +324,10 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     const Geo g = p.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int x0 = i0 - 4, y0 = j0 - 3;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the warp index through a shuffle from lane 0, so that the compiler
+    // treats every row condition below as warp-uniform (plain branches, no
+    // reconvergence bookkeeping)
+    const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
     const int X = 2 * lane;
     const int ia = x0 + X, ib = ia + 1;   // global x of the pair
     const CUtensorMap *mq = p.q0maps + s;
@@ -694,6 +718,11 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     const float2 fl = flux<EXACT>(qcl, qc, u2[r]), fr = rgt(fl);
                     if constexpr (INT && !EXACT) {
                         fct_pair_fast(qcl, qc, qcr, q0l, q0c, q0r, fl, fr, bxi[r], bxo[r]);
+                    } else if constexpr (!EXACT) {
+                        float2 a1m = qcl, a1p = qcr, a0m = q0l, a0c = q0c, a0p = q0r, afl = fl, afr = fr;
+                        fct_edge_sub(ia == 0, ia == nx - 1, a1m.x, qc.x, a1p.x, a0m.x, a0c.x, a0p.x, afl.x, afr.x);
+                        fct_edge_sub(ib == 0, ib == nx - 1, a1m.y, qc.y, a1p.y, a0m.y, a0c.y, a0p.y, afl.y, afr.y);
+                        fct_pair_fast(a1m, qc, a1p, a0m, a0c, a0p, afl, afr, bxi[r], bxo[r]);
                     } else {
                         const int pa = INT ? 0 : (ia == 0 ? 1 : (ia == nx - 1 ? 2 : 0));
                         const int pb = INT ? 0 : (ib == 0 ? 1 : (ib == nx - 1 ? 2 : 0));
@@ -711,6 +740,13 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     const float2 fl = flux<EXACT>(qs, qc, v2[r]), fr = flux<EXACT>(qc, qn, vn);
                     if constexpr (INT && !EXACT) {
                         fct_pair_fast(qs, qc, qn, q0s, q0c, q0n, fl, fr, byi[r], byo[r]);
+                    } else if constexpr (!EXACT) {
+                        float2 a1m = qs, a1p = qn, a0m = q0s, a0c = q0c, a0p = q0n, afl = fl, afr = fr;
+                        if (j == 0 || j == ny - 1) {   // row-uniform
+                            fct_edge_sub(j == 0, j == ny - 1, a1m.x, qc.x, a1p.x, a0m.x, a0c.x, a0p.x, afl.x, afr.x);
+                            fct_edge_sub(j == 0, j == ny - 1, a1m.y, qc.y, a1p.y, a0m.y, a0c.y, a0p.y, afl.y, afr.y);
+                        }
+                        fct_pair_fast(a1m, qc, a1p, a0m, a0c, a0p, afl, afr, byi[r], byo[r]);
                     } else {
                         const int pj = INT ? 0 : (j == 0 ? 1 : (j == ny - 1 ? 2 : 0));
                         fct_cell<EXACT>(qs.x, qc.x, qn.x, q0s.x, q0c.x, q0n.x, fl.x, fr.x, pj, false, byi[r].x,
