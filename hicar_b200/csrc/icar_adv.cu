@@ -759,7 +759,7 @@ int ensure_onepass(icar_adv_t *h)
     return ICAR_ADV_OK;
 }
 
-int onepass_tiles_x(const Geo &g) { return (g.nx + icar::op::TX - 1) / icar::op::TX; }
+int onepass_tiles_x(const Geo &g) { return icar::op::tiles_x(g.nx); }
 int onepass_tiles_y(const Geo &g) { return (g.ny + icar::op::TY - 1) / icar::op::TY; }
 
 // The corrective pass and the donor-cell pass for species [s0, s1) in one
@@ -1915,7 +1915,7 @@ int build_tables(icar_adv_batch_t *b)
             for (int s = 0; s < h->desc.n_species; s++)
                 for (int a = 0; a < tyn; a++)
                     for (int c = 0; c < tx; c++)
-                        items.push_back(make_int4(m, s, c * icar::op::TX, a * icar::op::TY));
+                        items.push_back(make_int4(m, s, c, a * icar::op::TY));
         } else {
             const int tx = icar::mp_tiles_x(g), tyn = icar::mp_tiles_y(g, ty);
             for (int s = 0; s < h->desc.n_species; s++)

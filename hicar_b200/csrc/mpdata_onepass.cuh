@@ -42,12 +42,12 @@
 namespace icar {
 
 namespace op {
-constexpr int PW = 64;               // plane width (floats): x from i0-4 to i0+59
+constexpr int PW = 64;               // plane width (floats): x from x0 to x0+63
 constexpr int PH = 32;               // plane rows: y from j0-3 to j0+28
 constexpr int NW = 16;               // warps per CTA
 constexpr int NT = NW * 32;
 constexpr int RPW = PH / NW;         // rows per warp (warp w owns rows w and w+NW)
-constexpr int TX = PW - 8;           // 56 output columns: plane x 4..59
+constexpr int TX = PW - 8;           // 56 output columns of an inner column tile: plane x 4..59
 constexpr int TY = PH - 6;           // 26 output rows: plane y 3..28
 constexpr int PLANE = PW * PH;
 constexpr uint32_t PLANE_BYTES = PLANE * sizeof(float);
@@ -65,6 +65,33 @@ constexpr int NPLANES = 25;
 constexpr size_t SMEM = (size_t)NPLANES * PLANE * sizeof(float) + 128;
 constexpr uint64_t WAIT_NS = 2000000000ull;  // a TMA wait gives up after 2 s
 constexpr int MAXS = 32;             // species per launch
+
+// Column tiles.  An inner tile's plane keeps 4 halo columns on each side
+// (56 output columns; the plane origin stays 16-byte aligned for TMA).  The
+// first and last tiles of a row sit on the domain's edges, where there is
+// nothing to read beyond the edge, so the first outputs the 60 columns from
+// x = 0 and the last ends at the domain's last column: nx = 512 takes 9
+// tiles where 56-column tiling takes 10.
+__host__ __device__ inline int tiles_x(int nx) { return nx <= PW ? 1 : 2 + max(0, (nx - 120 + TX - 1) / TX); }
+
+// Plane origin x0 and output columns [xlo, xhi) (plane coordinates) of
+// column tile tx of ntx.
+__device__ __forceinline__ void xtile(int nx, int tx, int ntx, int &x0, int &xlo, int &xhi)
+{
+    if (ntx == 1) {
+        x0 = 0, xlo = 0, xhi = nx;
+    } else if (tx == 0) {
+        x0 = 0, xlo = 0, xhi = PW - 4;
+    } else {
+        const int start = PW - 4 + TX * (tx - 1);   // first output column
+        if (tx < ntx - 1) {
+            x0 = start - 4, xlo = 4, xhi = PW - 4;
+        } else {
+            x0 = (nx - PW + 3) & ~3;               // the plane reaches the last column (at most 3 beyond)
+            xlo = start - x0, xhi = nx - x0;
+        }
+    }
+}
 }  // namespace op
 
 // Kernel parameters.  The tensor maps (64 x 1 x 32 boxes over (x, z, y))
@@ -317,13 +344,13 @@ __device__ __forceinline__ float2 cross_x(float2 v, float2 U, float2 ev, float2 
 // TMA wait gave up (the flag in p.err is then set and the CTA must stop).
 template <bool EXACT, bool FCT, bool INT>
 __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t *ph, const OnePassParams &p, int s,
-                                             int i0, int j0)
+                                             int x0, int xlo, int xhi, int j0)
 {
     using namespace op;
     using namespace opx;
     const Geo g = p.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int x0 = i0 - 4, y0 = j0 - 3;
+    const int y0 = j0 - 3;
     // the warp index through a shuffle from lane 0, so that the compiler
     // treats every row condition below as warp-uniform (plain branches, no
     // reconvergence bookkeeping)
@@ -635,11 +662,13 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                         // x cross term: the two rows' pair sums at x+1 and x-1, and U_m on the
                         // cells' west and east faces in both rows, each formed from one shuffle
                         const float2 sq = add2(qc, qs), yp = rgt(sq), ym = lft(sq);
-                        const float2 eq = mul2(sub2(yp, ym), rcp2(add2(add2(yp, ym), splat2(1e-10f))));
+                        float2 eq = mul2(sub2(yp, ym), rcp2(add2(add2(yp, ym), splat2(1e-10f))));
                         const float2 su = add2(Ut, Us);
                         float2 ev = add2(su, rgt(su));
-                        if (!xa) ev.x = 0.0f;
-                        if (!xb) ev.y = 0.0f;
+                        // no cross term on the domain's first and last columns (their
+                        // shuffled neighbours may lie outside the plane)
+                        if (!xa) ev.x = eq.x = 0.0f;
+                        if (!xb) ev.y = eq.y = 0.0f;
                         val = fma2(mul2(mc, ev), eq, val);
                         if (kint) {
                             const float2 zp = add2(ld2(Qu, Y, X), ld2(Qu, Y - 1, X));
@@ -865,8 +894,8 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                 }
                 const bool jin = INT || (j >= 0 && j < ny);
                 const bool jring = !INT && (j == 0 || j == ny - 1);
-                const bool oa = jin && (INT || inA) && X >= 4 && X < 4 + TX;
-                const bool ob = jin && (INT || inB) && X + 1 >= 4 && X + 1 < 4 + TX;
+                const bool oa = jin && (INT || inA) && X >= xlo && X < xhi;
+                const bool ob = jin && (INT || inB) && X + 1 >= xlo && X + 1 < xhi;
                 float va = val.x, vb = val.y;
                 if (!INT) {
                     const float2 q0L = ld2(sq0(L), Y, X);
@@ -915,10 +944,22 @@ __device__ __forceinline__ void onepass_init_bars(uint64_t *bars, uint32_t *ph)
     __syncthreads();
 }
 
-// Whether a tile's whole plane lies inside the domain interior.
-__device__ __forceinline__ bool onepass_interior(const Geo &g, int i0, int j0)
+// Whether a tile's whole plane (origin x0, first output row j0) lies inside
+// the domain interior.
+__device__ __forceinline__ bool onepass_interior(const Geo &g, int x0, int j0)
 {
-    return i0 - 4 >= 1 && i0 - 4 + op::PW - 1 <= g.nx - 2 && j0 - 3 >= 1 && j0 - 3 + op::PH - 1 <= g.ny - 2;
+    return x0 >= 1 && x0 + op::PW - 1 <= g.nx - 2 && j0 - 3 >= 1 && j0 - 3 + op::PH - 1 <= g.ny - 2;
+}
+
+// Tile (tx, j0) of a domain: plane origin and output columns, then the march.
+template <bool EXACT, bool FCT>
+__device__ __forceinline__ bool onepass_run(float *sm, uint64_t *bars, uint32_t *ph, const OnePassParams &p, int s,
+                                            int tx, int j0)
+{
+    int x0, xlo, xhi;
+    op::xtile(p.g.nx, tx, p.tiles_x, x0, xlo, xhi);
+    if (onepass_interior(p.g, x0, j0)) return onepass_tile<EXACT, FCT, true>(sm, bars, ph, p, s, x0, xlo, xhi, j0);
+    return onepass_tile<EXACT, FCT, false>(sm, bars, ph, p, s, x0, xlo, xhi, j0);
 }
 
 template <bool EXACT, bool FCT>
@@ -931,18 +972,17 @@ __global__ void __launch_bounds__(op::NT, 1) k_mpdata_onepass(const __grid_const
     __shared__ __align__(8) uint64_t bars[2];
     const int s = blockIdx.x % p.nspecies;
     const int tile = blockIdx.x / p.nspecies;
-    const int i0 = (tile % p.tiles_x) * TX, j0 = (tile / p.tiles_x) * TY;
+    const int tx = tile % p.tiles_x, j0 = (tile / p.tiles_x) * TY;
     __shared__ int stop;
     if (threadIdx.x == 0) stop = *reinterpret_cast<volatile const int *>(p.err);
     __syncthreads();
     if (stop) return;   // an earlier tile of this launch gave up on a TMA wait: stop (the whole CTA)
     uint32_t ph[2];
     onepass_init_bars(bars, ph);
-    if (onepass_interior(p.g, i0, j0)) onepass_tile<EXACT, FCT, true>(sm, bars, ph, p, s, i0, j0);
-    else onepass_tile<EXACT, FCT, false>(sm, bars, ph, p, s, i0, j0);
+    onepass_run<EXACT, FCT>(sm, bars, ph, p, s, tx, j0);
 }
 
-// Batched form: persistent CTAs (one per SM) pull (member, species, i0, j0)
+// Batched form: persistent CTAs (one per SM) pull (member, species, tx, j0)
 // items from a work list with an atomic counter; params[member] holds that
 // member's descriptors, pointers and geometry for the current buffer parity.
 template <bool EXACT, bool FCT>
@@ -974,10 +1014,7 @@ __global__ void __launch_bounds__(op::NT, 1)
         const int *src = reinterpret_cast<const int *>(params + w.x);
         for (int q = threadIdx.x; q < PW4; q += blockDim.x) reinterpret_cast<int *>(&sp)[q] = src[q];
         __syncthreads();
-        bool fine;
-        if (onepass_interior(sp.g, w.z, w.w)) fine = onepass_tile<EXACT, FCT, true>(sm, bars, ph, sp, w.y, w.z, w.w);
-        else fine = onepass_tile<EXACT, FCT, false>(sm, bars, ph, sp, w.y, w.z, w.w);
-        if (!fine) break;  // the barriers' phases are no longer known: this CTA stops
+        if (!onepass_run<EXACT, FCT>(sm, bars, ph, sp, w.y, w.z, w.w)) break;  // the barriers' phases are no longer known: this CTA stops
         __syncthreads();   // every thread is done with the planes and parameters before the next tile
     }
 }
