@@ -506,8 +506,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
             else val = sub2x(val, div2x(sub2x(mul2x(c, wtop), vb), djr));
         } else {
             const float2 vdiv = mid ? sub2(vt, vb) : (L == 0 ? vt : sub2(mul2(c, wtop), vb));
-            val = fma2(make_float2(-hd.x, -hd.y), rcp2(G), c);
-            val = fma2(make_float2(-vdiv.x, -vdiv.y), rcp2(djr), val);
+            val = sub2(sub2(c, mul2(hd, rcp2(G))), mul2(vdiv, rcp2(djr)));
         }
         float2 q1 = val;
         if (!INT) {
@@ -853,7 +852,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                 const float2 hd = ad<EXACT>(sb<EXACT>(fe, fw), sb<EXACT>(f3, f4));
                 const float2 G = ld2(sG(t), Y, X);
                 if constexpr (EXACT) n_part = sub2x(qc, div2x(hd, G));
-                else n_part = fma2(make_float2(-hd.x, -hd.y), rcp2(G), qc);
+                else n_part = sub2(qc, mul2(hd, rcp2(G)));
                 if (t >= 1) {
                     const float2 qd = ld2(sQ1(t - 1), Y, X);
                     if constexpr (EXACT) {
@@ -890,7 +889,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     if (L > 0 && L < nz - 1) vd = sub2(n_ft, r_fb[r]);
                     else if (L == 0) vd = n_ft;
                     else vd = make_float2(-r_fb[r].x, -r_fb[r].y);   // nothing leaves through the model top
-                    val = fma2(make_float2(-vd.x, -vd.y), rcp2(djr), val);
+                    val = sub2(val, mul2(vd, rcp2(djr)));
                 }
                 const bool jin = INT || (j >= 0 && j < ny);
                 const bool jring = !INT && (j == 0 || j == ny - 1);
