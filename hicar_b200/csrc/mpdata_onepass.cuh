@@ -453,17 +453,25 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     const size_t lstride = (size_t)g.P;
 
     // own-column values by plain loads, one level ahead
+    // (the fast variant carries dz*J*rho as its reciprocal: each value
+    // divides twice, in the donor pass and in the corrective pass)
     float2 r_wm[RPW], n_wm[RPW], r_djr0[RPW], r_djrm[RPW], n_djr[RPW], n_dz[RPW];
-    // carried z state of the output cells, and the donor pass's flux
-    // through the top of the level it formed last
-    float2 r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_fb[RPW], r_part[RPW], r_vt[RPW];
+    auto djr_in = [](float2 v) -> float2 {
+        if constexpr (EXACT) return v;
+        else return rcp2(v);
+    };
+    // carried z state of the output cells, the donor pass's flux through
+    // the top of the level it formed last, and (fast variant) the
+    // reciprocal of J*rho that the donor pass formed for the level the
+    // corrective pass updates next (r_rg: level t, n_rg: level t+1)
+    float2 r_w2[RPW], r_bzi[RPW], r_bzo[RPW], r_fb[RPW], r_part[RPW], r_vt[RPW], r_rg[RPW], n_rg[RPW];
     auto ldcol = [&](const float *src, int r, int lev) -> float2 {
         return *reinterpret_cast<const float2 *>(src + rowc[r] + (size_t)lev * lstride);
     };
 #pragma unroll
     for (int r = 0; r < RPW; r++) {
         r_wm[r] = ldcol(p.Wm, r, 0);
-        r_djr0[r] = ldcol(p.DJR, r, 0);
+        r_djr0[r] = djr_in(ldcol(p.DJR, r, 0));
         n_wm[r] = nz > 1 ? ldcol(p.Wm, r, 1) : splat2(0.0f);
         n_djr[r] = nz > 1 ? ldcol(p.DJR, r, 1) : splat2(1.0f);
         n_dz[r] = ldcol(p.dz, r, 0);
@@ -474,9 +482,9 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
     const float2 zero2 = splat2(0.0f);
 
     // ---- P0: donor-cell pass at level L into the q1 plane of L ----------
-    // wtop = W_m(L), djr = dz*J*rho at L, own pair.  Levels are formed in
-    // order, so the flux through the bottom of L is the one through the top
-    // of L-1, carried in r_vt.
+    // wtop = W_m(L), djr = dz*J*rho at L (its reciprocal in the fast
+    // variant), own pair.  Levels are formed in order, so the flux through
+    // the bottom of L is the one through the top of L-1, carried in r_vt.
     auto donor = [&](int L, int r, float2 wtop, float2 djr) {
         const int Y = rowY[r], j = rowj[r];
         const bool need = Y >= 1 && Y <= PH - 2;     // warp-uniform
@@ -506,7 +514,9 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
             else val = sub2x(val, div2x(sub2x(mul2x(c, wtop), vb), djr));
         } else {
             const float2 vdiv = mid ? sub2(vt, vb) : (L == 0 ? vt : sub2(mul2(c, wtop), vb));
-            val = sub2(sub2(c, mul2(hd, rcp2(G))), mul2(vdiv, rcp2(djr)));
+            const float2 rg = rcp2(G);
+            n_rg[r] = rg;
+            val = sub2(sub2(c, mul2(hd, rg)), mul2(vdiv, djr));
         }
         float2 q1 = val;
         if (!INT) {
@@ -536,7 +546,8 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
 #pragma unroll
         for (int r = 0; r < RPW; r++) {
             c_wmn[r] = n_wm[r];
-            c_djrn[r] = n_djr[r];
+            c_djrn[r] = djr_in(n_djr[r]);
+            r_rg[r] = n_rg[r];
             c_dz[r] = n_dz[r];
             if (t + 2 < nz) {
                 n_wm[r] = ldcol(p.Wm, r, t + 2);
@@ -852,7 +863,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                 const float2 hd = ad<EXACT>(sb<EXACT>(fe, fw), sb<EXACT>(f3, f4));
                 const float2 G = ld2(sG(t), Y, X);
                 if constexpr (EXACT) n_part = sub2x(qc, div2x(hd, G));
-                else n_part = sub2(qc, mul2(hd, rcp2(G)));
+                else n_part = sub2(qc, mul2(hd, r_rg[r]));
                 if (t >= 1) {
                     const float2 qd = ld2(sQ1(t - 1), Y, X);
                     if constexpr (EXACT) {
@@ -889,7 +900,7 @@ __device__ __forceinline__ bool onepass_tile(float *sm, uint64_t *bars, uint32_t
                     if (L > 0 && L < nz - 1) vd = sub2(n_ft, r_fb[r]);
                     else if (L == 0) vd = n_ft;
                     else vd = make_float2(-r_fb[r].x, -r_fb[r].y);   // nothing leaves through the model top
-                    val = sub2(val, mul2(vd, rcp2(djr)));
+                    val = sub2(val, mul2(vd, djr));
                 }
                 const bool jin = INT || (j >= 0 && j < ny);
                 const bool jring = !INT && (j == 0 || j == ny - 1);
