@@ -363,7 +363,7 @@ __device__ __forceinline__ void mp_corr_tile(float *sm, const Geo &g, const floa
     constexpr int TY = SH::TY, NW = SH::NW, PH = SH::PH, PLANE = SH::PLANE, RPW = SH::RPW;
     (void)PH;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
     const float e10 = 1e-10f, e15 = 1e-15f, q4 = 1.0f / 4.0f;
     auto P = [&](int slot) { return sm + (size_t)slot * PLANE; };
 #define AT(slot, lx, ly) sm[(size_t)(slot) * PLANE + (ly) * PW + (lx)]
