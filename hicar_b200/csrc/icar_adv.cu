@@ -1962,7 +1962,7 @@ int build_tables(icar_adv_batch_t *b)
         }
     }
     // longest columns first (cost ~ nz per tile), so the tail of the
-    // persistent launch is made of short items
+    // launch is made of short items
     std::stable_sort(items.begin(), items.end(), [&](const int4 &x, const int4 &y) {
         return b->members[x.x]->g.nz > b->members[y.x]->g.nz;
     });
@@ -2034,7 +2034,9 @@ int build_tables(icar_adv_batch_t *b)
     if (seg[7]) BCUDA(b, cudaMemcpyAsync(b->d_bmaps, st + off[7], seg[7], cudaMemcpyHostToDevice, b->stream));
     BCUDA(b, cudaEventRecord(b->stage_done[t], b->stream));
     b->stage_turn ^= 1;
-    b->ctas = onepass ? std::min(std::max(b->n_items, 1), b->nsm)  // one 192 KB CTA per SM
+    // the single-pass launch has one CTA per item; the two-pass correction
+    // kernel is persistent
+    b->ctas = onepass ? b->n_items
                       : std::min(std::max(b->n_items, 1), icar::batch_corr_max_ctas(b->shape, b->fct, b->nsm));
     b->tables_dirty = false;
     return ICAR_ADV_OK;
@@ -2049,16 +2051,15 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
         icar::k_batch_forcing<<<b->n_force, 256, 0, st>>>(mem, b->d_ints + b->off_f, b->d_pairs, b->n_pairs);
     if (b->n_prep > 0) icar::k_batch_prep<<<b->n_prep, 256, 0, st>>>(mem, b->d_ints, M);
     if (b->path >= 2) {
-        cudaMemsetAsync(b->d_ints + b->off_counter, 0, sizeof(int), st);
         if (b->n_items > 0) {
             const icar::OnePassParams *opp = b->d_opp[p];
-            int *ctr = b->d_ints + b->off_counter;
-            const int n = b->n_items, c = b->ctas;
+            const int n = b->n_items;
             const size_t sm = icar::op::SMEM;
-            if (b->path == 2 && b->fct) icar::k_batch_onepass<true, true><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
-            else if (b->path == 2) icar::k_batch_onepass<true, false><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
-            else if (b->fct) icar::k_batch_onepass<false, true><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
-            else icar::k_batch_onepass<false, false><<<c, icar::op::NT, sm, st>>>(opp, b->d_items, n, ctr);
+            const int4 *it = b->d_items;
+            if (b->path == 2 && b->fct) icar::k_batch_onepass_items<true, true><<<n, icar::op::NT, sm, st>>>(opp, it);
+            else if (b->path == 2) icar::k_batch_onepass_items<true, false><<<n, icar::op::NT, sm, st>>>(opp, it);
+            else if (b->fct) icar::k_batch_onepass_items<false, true><<<n, icar::op::NT, sm, st>>>(opp, it);
+            else icar::k_batch_onepass_items<false, false><<<n, icar::op::NT, sm, st>>>(opp, it);
         }
         return;
     }
@@ -2074,13 +2075,14 @@ void enqueue_step(icar_adv_batch_t *b, int p, cudaStream_t st)
 cudaError_t batch_onepass_setup()
 {
     const int sm = (int)icar::op::SMEM;
-    cudaError_t e = cudaFuncSetAttribute(icar::k_batch_onepass<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaError_t e =
+        cudaFuncSetAttribute(icar::k_batch_onepass_items<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(icar::k_batch_onepass<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        e = cudaFuncSetAttribute(icar::k_batch_onepass_items<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(icar::k_batch_onepass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        e = cudaFuncSetAttribute(icar::k_batch_onepass_items<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(icar::k_batch_onepass<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        e = cudaFuncSetAttribute(icar::k_batch_onepass_items<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     return e;
 }
 

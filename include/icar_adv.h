@@ -280,8 +280,10 @@ int icar_adv_profile_read_correction(icar_adv_t *h, double *ms, int64_t *launche
  * per process).  Many independent domains -- ensemble members or served
  * requests of uneven nx x ny x nz -- advance together: one step is a single
  * CUDA-graph launch holding the boundary update, the per-step wind fields,
- * the donor-cell pass and one persistent correction kernel over a
- * (member, species, tile) work list.  Each member keeps its own device
+ * the donor-cell pass and one correction kernel over a (member, species,
+ * tile) work list (two-pass kernels, persistent CTAs), or one single-pass
+ * launch over that work list with one CTA per item (icar_adv_batch_set_path
+ * 2 or 3).  Each member keeps its own device
  * fields; while it is a member its work runs on the batch's stream, it
  * cannot be stepped on its own, and set/get_field stay available.  All
  * members must use MPDATA order 2 without RK3 and share MPDATA_FCT.
