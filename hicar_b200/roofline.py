@@ -87,9 +87,9 @@ def correction_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launch
 
 
 # DRAM bytes (read + write) per cell-species of one k_mpdata_onepass launch
-# (fast variant, FCT on), from an ncu capture of a 256x256x40, 12-species
-# launch: 227.97 MB read + 103.27 MB written for 31.46 M cell-species.
-ONEPASS_DRAM_BYTES_PER_CS = (227.970048e6 + 103.272448e6) / (256 * 256 * 40 * 12)
+# (fast variant, FCT on), from an ncu capture of the 512x512x40, 12-species
+# bench launch: 955.92 MB read + 483.57 MB written for 125.8 M cell-species.
+ONEPASS_DRAM_BYTES_PER_CS = (955.918592e6 + 483.570688e6) / (512 * 512 * 40 * 12)
 
 
 def single_pass_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launches: int) -> dict:
@@ -107,5 +107,5 @@ def single_pass_kernel(nx: int, ny: int, nz: int, S: int, total_ms: float, launc
         "launch_ms": (total_ms / launches) if launches else None,
         "bytes_model": "8 + 28/S B per cell-species; one launch = all species of one advect call",
         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per cell-species of a "
-                           "256x256x40x12 launch, scaled to this launch by cell-species"),
+                           "512x512x40x12 launch, scaled to this launch by cell-species"),
     }
