@@ -103,3 +103,21 @@ def test_fast_closed_domain_mass():
     m = lambda q: float((q.astype(np.float64) * case.jacobian * case.density * case.advection_dz).sum())
     out = run_fast(case, 50)
     assert abs(m(out["qv"]) - m(case.species["qv"])) / m(case.species["qv"]) < 2e-6
+
+
+def test_fast_no_new_negatives(oracle_lib):
+    """Where the FP32 oracle (the reference's arithmetic) stays non-negative
+    over 5 MPDATA + FCT steps, so does the fast kernel, up to rounding at
+    the field's scale (>= -1e-6 max|q|).  The reference's limiter makes no
+    exact positivity promise in 3-D (its FCT is one-dimensional per
+    direction); the exact promise, for the donor-cell pass, is checked on
+    the bit-exact kernels (tests/test_parity_gpu.py)."""
+    O = oracle_lib
+    case = synth.config2(seed=6, nx=64, ny=48, nz=16)
+    case.species = {k: case.species[k] for k in ("qc", "qr", "nr")}
+    ref = O.run_steps(case, O.make_opts(), case.dt, 5)
+    out = run_fast(case, 5)
+    for k in ref:
+        scale = float(np.abs(ref[k]).max())
+        bad = (ref[k] >= 0) & (out[k] < -1e-6 * scale)
+        assert not bad.any(), (k, int(bad.sum()), float(out[k][bad].min()))
