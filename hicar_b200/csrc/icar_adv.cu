@@ -215,13 +215,67 @@ int64_t footprint_bytes(const icar_adv_desc &d, const icar_adv_opts &o)
     return total;
 }
 
+// Device memory of the handles comes from one stream-ordered memory pool
+// per device that keeps freed memory for reuse (its release threshold is
+// never reached).  Creating and destroying a handle then neither maps nor
+// unmaps device memory, and destroying one does not wait for the device
+// (cudaFree waits for every launch on the device): a request server that
+// admits and retires many domains a second while its batched steps run
+// depends on both.  Allocations are ordered on the handle's stream; the
+// frees are ordered on it too, after all the work queued there.
+constexpr int POOL_MAX_DEVICES = 64;
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pool[POOL_MAX_DEVICES] = {};
+
+cudaError_t pool_of(int dev, cudaMemPool_t *out)
+{
+    if (dev < 0 || dev >= POOL_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = UINT64_MAX;
+        e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        g_pool[dev] = p;
+    }
+    *out = g_pool[dev];
+    return cudaSuccess;
+}
+
+// bytes of device memory for handle h, ordered on its stream
+cudaError_t dev_alloc(icar_adv_t *h, void **p, size_t bytes)
+{
+    cudaMemPool_t pool;
+    cudaError_t e = pool_of(h->desc.device, &pool);
+    if (e != cudaSuccess) return e;
+    e = cudaMallocFromPoolAsync(p, bytes, pool, h->stream);
+    if (e != cudaSuccess) *p = nullptr;
+    return e;
+}
+
+void dev_free(void *p, cudaStream_t st)
+{
+    if (p) cudaFreeAsync(p, st);
+}
+
 int alloc(icar_adv_t *h, DevBuf &b, size_t n)
 {
     if (b.p) return ICAR_ADV_OK;
-    cudaError_t e = cudaMalloc(&b.p, n * sizeof(float));
+    cudaError_t e = dev_alloc(h, (void **)&b.p, n * sizeof(float));
     if (e != cudaSuccess) {
         b.p = nullptr;
-        return fail(h, ICAR_ADV_OOM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(float), cudaGetErrorString(e));
+        return fail(h, e == cudaErrorMemoryAllocation ? ICAR_ADV_OOM : ICAR_ADV_CUDA_ERROR,
+                    "device allocation of %zu bytes failed: %s", n * sizeof(float), cudaGetErrorString(e));
     }
     b.n = n;
     h->bytes += n * sizeof(float);
@@ -230,9 +284,9 @@ int alloc(icar_adv_t *h, DevBuf &b, size_t n)
     return ICAR_ADV_OK;
 }
 
-void release(DevBuf &b)
+void release(DevBuf &b, cudaStream_t st)
 {
-    if (b.p) cudaFree(b.p);
+    dev_free(b.p, st);
     b.p = nullptr;
     b.n = 0;
 }
@@ -298,18 +352,24 @@ int upload_filter(icar_adv_t *h)
     for (int j = 0; j < h->g.ny; j++)
         for (int i = 0; i < h->g.nx; i++)
             if (h->filter_host[(size_t)i + (size_t)h->g.nx * j] != 0.0f) zone.push_back(i + h->g.nx * j);
-    if (h->zone_dev) { cudaFree(h->zone_dev); h->zone_dev = nullptr; }
+    if (h->zone_dev) {
+        dev_free(h->zone_dev, h->stream);
+        h->zone_dev = nullptr;
+    }
     h->nzone = (int)zone.size();
     if (!h->filter_dev) {
-        CUDA_TRY(h, cudaMalloc(&h->filter_dev, sizeof(float) * h->filter_host.size()));
+        CUDA_TRY(h, dev_alloc(h, (void **)&h->filter_dev, sizeof(float) * h->filter_host.size()));
         h->bytes += sizeof(float) * h->filter_host.size();
     }
-    CUDA_TRY(h, cudaMemcpy(h->filter_dev, h->filter_host.data(), sizeof(float) * h->filter_host.size(),
-                           cudaMemcpyHostToDevice));
+    CUDA_TRY(h, cudaMemcpyAsync(h->filter_dev, h->filter_host.data(), sizeof(float) * h->filter_host.size(),
+                                cudaMemcpyHostToDevice, h->stream));
     if (h->nzone > 0) {
-        CUDA_TRY(h, cudaMalloc(&h->zone_dev, sizeof(int) * zone.size()));
-        CUDA_TRY(h, cudaMemcpy(h->zone_dev, zone.data(), sizeof(int) * zone.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(h, dev_alloc(h, (void **)&h->zone_dev, sizeof(int) * zone.size()));
+        CUDA_TRY(h, cudaMemcpyAsync(h->zone_dev, zone.data(), sizeof(int) * zone.size(), cudaMemcpyHostToDevice,
+                                    h->stream));
     }
+    // the host vectors are the copies' sources
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return ICAR_ADV_OK;
 }
 
@@ -708,7 +768,7 @@ int onepass_maps(icar_adv_t *h, const CUtensorMap **out)
         }
     const int t = h->map_next;
     h->map_next ^= 1;
-    if (!h->map_dev[t]) CUDA_TRY(h, cudaMalloc(&h->map_dev[t], (size_t)(S + 4) * sizeof(CUtensorMap)));
+    if (!h->map_dev[t]) CUDA_TRY(h, dev_alloc(h, (void **)&h->map_dev[t], (size_t)(S + 4) * sizeof(CUtensorMap)));
     std::vector<CUtensorMap> host(S + 4);
     int e;
     const CUtensorMap *m;
@@ -748,7 +808,7 @@ int ensure_onepass(icar_adv_t *h)
         for (int s = 0; s < S; s++)
             if ((e = alloc(h, h->qn[s], h->n_cell))) return e;
         if (!h->op_err) {
-            CUDA_TRY(h, cudaMalloc(&h->op_err, sizeof(int)));
+            CUDA_TRY(h, dev_alloc(h, (void **)&h->op_err, sizeof(int)));
             CUDA_TRY(h, cudaMemsetAsync(h->op_err, 0, sizeof(int), h->stream));
         }
         cudaError_t ce = onepass_attr<true>();
@@ -1138,35 +1198,39 @@ int icar_adv_destroy(icar_adv_t *h)
     if (!h) return ICAR_ADV_OK;
     if (h->batch) icar_adv_batch_remove(h->batch, h);
     cudaSetDevice(h->desc.device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
+    // copies through the caller's host buffers end before this returns
+    if (h->io_in) cudaStreamSynchronize(h->io_in);
+    if (h->io_out) cudaStreamSynchronize(h->io_out);
+    // The device memory goes back to the pool in the order of the handle's
+    // stream, after all the work queued there (a former batch member's
+    // stream waits for the batch launches queued before its removal), so
+    // nothing here waits for the device.
+    cudaStream_t st = h->stream;
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
                       &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
                       &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp, &h->Gc,
                       &h->DJR, &h->Wp, &h->dtbuf, &h->pressure, &h->exner, &h->dz_mass, &h->dz_interface})
-        release(*b);
-    if (h->acc_precip) cudaFree(h->acc_precip);
-    if (h->mp_stop) cudaFree(h->mp_stop);
-    if (h->op_err) cudaFree(h->op_err);
-    for (auto *m : h->map_dev)
-        if (m) cudaFree(m);
-    for (auto &b : h->q) release(b);
-    for (auto &b : h->qn) release(b);
-    for (auto &b : h->q1s) release(b);
+        release(*b, st);
+    dev_free(h->acc_precip, st);
+    dev_free(h->mp_stop, st);
+    dev_free(h->op_err, st);
+    for (auto *m : h->map_dev) dev_free(m, st);
+    for (auto &b : h->q) release(b, st);
+    for (auto &b : h->qn) release(b, st);
+    for (auto &b : h->q1s) release(b, st);
+    for (auto &b : h->forcing) release(b, st);
+    for (auto &b : h->dqdt) release(b, st);
+    dev_free(h->filter_dev, st);
+    dev_free(h->zone_dev, st);
     for (auto *v : {&h->events, &h->corr_events})
         for (auto &p : *v) {
             cudaEventDestroy(p.first);
             cudaEventDestroy(p.second);
         }
-    for (auto &b : h->forcing) release(b);
-    for (auto &b : h->dqdt) release(b);
-    if (h->filter_dev) cudaFree(h->filter_dev);
-    if (h->zone_dev) cudaFree(h->zone_dev);
-    if (h->io_in) cudaStreamSynchronize(h->io_in);
-    if (h->io_out) cudaStreamSynchronize(h->io_out);
     for (cudaEvent_t ev : h->io_events) cudaEventDestroy(ev);
     if (h->io_in) cudaStreamDestroy(h->io_in);
     if (h->io_out) cudaStreamDestroy(h->io_out);
-    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);   // its queued frees still run
     delete h;
     return ICAR_ADV_OK;
 }
@@ -1386,11 +1450,11 @@ int icar_adv_mp_simple(icar_adv_t *h, float dt)
     if (g.nz > 512) return fail(h, ICAR_ADV_BAD_ARG, "mp_simple supports at most 512 levels");
     const size_t n2 = (size_t)g.nx * g.ny;
     if (!h->acc_precip) {
-        CUDA_TRY(h, cudaMalloc(&h->acc_precip, 2 * n2 * sizeof(double)));
+        CUDA_TRY(h, dev_alloc(h, (void **)&h->acc_precip, 2 * n2 * sizeof(double)));
         CUDA_TRY(h, cudaMemsetAsync(h->acc_precip, 0, 2 * n2 * sizeof(double), h->stream));
     }
     if (!h->mp_stop) {
-        CUDA_TRY(h, cudaMalloc(&h->mp_stop, sizeof(int)));
+        CUDA_TRY(h, dev_alloc(h, (void **)&h->mp_stop, sizeof(int)));
         CUDA_TRY(h, cudaMemsetAsync(h->mp_stop, 0, sizeof(int), h->stream));
     }
     // the time constants of this dt, in the reference's FP32 (mp_simple.f90:618-622)
@@ -1429,7 +1493,7 @@ int icar_adv_set_precipitation(icar_adv_t *h, const double *rain, const double *
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
     cudaSetDevice(h->desc.device);
     const size_t n2 = (size_t)h->g.nx * h->g.ny;
-    if (!h->acc_precip) CUDA_TRY(h, cudaMalloc(&h->acc_precip, 2 * n2 * sizeof(double)));
+    if (!h->acc_precip) CUDA_TRY(h, dev_alloc(h, (void **)&h->acc_precip, 2 * n2 * sizeof(double)));
     for (int part = 0; part < 2; part++) {
         const double *src = part == 0 ? rain : snow;
         double *dst = h->acc_precip + part * n2;

@@ -111,6 +111,9 @@ class Server:
         # the batch runs on this stream; completion times come from events on it
         self.stream = torch.cuda.Stream(device) if stream is None else torch.cuda.ExternalStream(stream, device)
         self.batch.set_stream(self.stream.cuda_stream)
+        # requests are generated and set up on a stream of their own: set-up
+        # waits for its own work, never for the batched steps in flight
+        self.setup_stream = torch.cuda.Stream(device)
         self._ev0 = None
         self.queue: collections.deque[Request] = collections.deque()
         self.live: list[_Live] = []
@@ -134,6 +137,8 @@ class Server:
 
     # -- admission ----------------------------------------------------------
     def _admit(self) -> None:
+        import torch
+
         from .synth import device_member
         now = self.now()
         while self.queue and self.queue[0].arrival <= now:
@@ -144,12 +149,13 @@ class Server:
             req.admitted = self.now()
             dom = None
             try:
-                fields, dt = device_member(req.nx, req.ny, req.nz, req.seed, device=self.device,
-                                           species=req.species)
-                dom = Domain.create_on_device(fields, req.nx, req.ny, req.nz, 4000.0, self.options,
-                                              device=self.device, forcing=True)
-                dom._device_fields = None      # the handle holds its own copies now
-                del fields
+                with torch.cuda.stream(self.setup_stream):
+                    fields, dt = device_member(req.nx, req.ny, req.nz, req.seed, device=self.device,
+                                               species=req.species)
+                    dom = Domain.create_on_device(fields, req.nx, req.ny, req.nz, 4000.0, self.options,
+                                                  device=self.device, forcing=True)
+                    dom._device_fields = None      # the handle holds its own copies now
+                    del fields
                 dom.set_path(self.path)
                 if self.fault_hook is not None:
                     self.fault_hook(req, "setup", 0)
