@@ -184,8 +184,8 @@ class Server:
             self.batch.sync()
             req.result = {k: t.cpu().numpy().reshape(req.ny, req.nz, req.nx) for k, t in out.items()}
         self.batch.remove(lv.dom)
-        # freeing device memory synchronises the device, so retired domains
-        # are destroyed in bulk (their memory stays counted until then)
+        # retired domains are destroyed in groups (their memory stays counted
+        # until then); destroy returns their memory in stream order
         self.graveyard.append((lv.dom, req.footprint))
         if len(self.graveyard) >= self.flush_every or (self.queue and self.used + self.queue[0].footprint > self.budget):
             self._flush_graveyard()
