@@ -145,6 +145,10 @@ int icar_adv_halo_size(const icar_adv_opts *opts);
  * handle, allocate the resident device fields, build the relaxation filter
  * (init_relax_filters, src/objects/domain_obj.f90:3285-3400). */
 int icar_adv_create(const icar_adv_desc *desc, const icar_adv_opts *opts, icar_adv_t **out);
+/* Release a handle.  Its device memory goes back to a pool the library keeps
+ * per device, in the order of the handle's stream (after the work queued
+ * there), without waiting for the device; the pool reuses it for later
+ * handles and holds it until the process exits. */
 int icar_adv_destroy(icar_adv_t *h);
 
 /* Copy one field between the host and the handle's resident device copy.
