@@ -18,8 +18,9 @@
 //
 // Data movement.  The level planes of q0 and of the per-step fields (U_m,
 // V_m, W_m/dz, J*rho) arrive in shared memory by TMA (64 x 32 boxes of
-// this GPU's own arrays, no multicast) one level ahead of use, completing on
-// mbarriers; W_m, dz*J*rho and dz of the thread's own columns come by plain
+// this GPU's own arrays, each CTA loading its own) one level ahead of use,
+// completing on mbarriers; W_m, dz*J*rho and dz of the thread's own columns
+// come by plain
 // loads one level ahead.  Each thread owns an x-pair of columns in two rows
 // and works on the pair with packed f32x2 arithmetic; x neighbours come by
 // warp shuffles, y neighbours from the shared planes.

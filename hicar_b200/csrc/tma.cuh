@@ -2,8 +2,8 @@
 // the single-pass MPDATA kernel, plus packed two-lane FP32 arithmetic.
 //
 // Every TMA load here reads this GPU's own memory with a tiled
-// cp.async.bulk.tensor copy (no cluster multicast), completing on an
-// mbarrier in the issuing CTA's shared memory.  Waits are bounded: a wait
+// cp.async.bulk.tensor copy into the issuing CTA's own shared memory only,
+// completing on an mbarrier there.  Waits are bounded: a wait
 // that gives up sets a flag in global memory that the host reads, so a
 // copy that never lands cannot hang the GPU.
 #pragma once
