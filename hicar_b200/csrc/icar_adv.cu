@@ -1202,10 +1202,23 @@ int icar_adv_destroy(icar_adv_t *h)
     if (h->io_in) cudaStreamSynchronize(h->io_in);
     if (h->io_out) cudaStreamSynchronize(h->io_out);
     // The device memory goes back to the pool in the order of the handle's
-    // stream, after all the work queued there (a former batch member's
-    // stream waits for the batch launches queued before its removal), so
-    // nothing here waits for the device.
-    cudaStream_t st = h->stream;
+    // own stream, after all the work queued on the stream it runs on (a
+    // former batch member's own stream already waits for the batch launches
+    // queued before its removal), so nothing here waits for the device.  If
+    // the handle ran on a caller's stream that is gone, the device is
+    // synchronised instead.
+    cudaStream_t st = h->own_stream;
+    if (h->stream != h->own_stream) {
+        cudaEvent_t ev = nullptr;
+        bool ordered = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess &&
+                       cudaEventRecord(ev, h->stream) == cudaSuccess &&
+                       cudaStreamWaitEvent(st, ev, 0) == cudaSuccess;
+        if (ev) cudaEventDestroy(ev);
+        if (!ordered) {
+            cudaGetLastError();
+            cudaDeviceSynchronize();
+        }
+    }
     for (DevBuf *b : {&h->u, &h->v, &h->w, &h->rho, &h->jac, &h->jac_u, &h->jac_v, &h->jac_w, &h->dz, &h->Um,
                       &h->Vm, &h->Wm, &h->spare, &h->q1, &h->u2, &h->v2, &h->w2, &h->u2l, &h->v2l, &h->w2l, &h->fx,
                       &h->fy, &h->fz, &h->ufx, &h->ufy, &h->ufz, &h->dq, &h->sin_, &h->sout, &h->temp, &h->Gc,
@@ -1684,7 +1697,19 @@ int icar_adv_sync_timeout(icar_adv_t *h, double timeout_s)
 int icar_adv_set_stream(icar_adv_t *h, void *cuda_stream)
 {
     if (!h) return fail(nullptr, ICAR_ADV_BAD_ARG, "handle is NULL");
-    h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    cudaStream_t next = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+    if (next != h->stream) {
+        // the handle's work stays in order across the switch: the new stream
+        // waits for what is queued on the old one (no host wait)
+        cudaSetDevice(h->desc.device);
+        cudaEvent_t ev = nullptr;
+        CUDA_TRY(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaError_t e = cudaEventRecord(ev, h->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(next, ev, 0);
+        cudaEventDestroy(ev);
+        if (e != cudaSuccess) return fail(h, ICAR_ADV_CUDA_ERROR, "stream switch: %s", cudaGetErrorString(e));
+    }
+    h->stream = next;
     return ICAR_ADV_OK;
 }
 

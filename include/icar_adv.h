@@ -254,7 +254,9 @@ int icar_adv_sync(icar_adv_t *h);
 int icar_adv_sync_timeout(icar_adv_t *h, double timeout_s);
 
 /* Use an external CUDA stream (cudaStream_t passed as void*; NULL = the
- * handle's own stream). */
+ * handle's own stream).  Work already queued on the previous stream comes
+ * first: the new stream waits for it (no host wait).  The stream must stay
+ * valid while the handle uses it. */
 int icar_adv_set_stream(icar_adv_t *h, void *cuda_stream);
 
 /* Bytes of device memory the handle holds. */

@@ -41,3 +41,29 @@ def test_destroy_with_queued_work_then_reuse(oracle_lib, path):
         got = _run(case, 3, path)           # may reuse that memory
         for k in want:
             assert np.array_equal(got[k], want[k]), k
+
+
+def test_destroy_on_caller_stream_then_reuse(oracle_lib):
+    """The same on a caller's stream (icar_adv_set_stream), switched to
+    while the handle's own stream still has its upload queued."""
+    import ctypes as C
+
+    import torch
+
+    from hicar_b200 import _lib as L
+    case = synth.config2(seed=22, nx=100, ny=70, nz=16)
+    ref = oracle_lib.run_steps(case, oracle_lib.make_opts(), case.dt, 3)
+    lib = L.load()
+    st = torch.cuda.Stream()
+    for _ in range(3):
+        d = Domain.from_case(case)
+        opts = Options()
+        adv_init(d, opts)
+        L.check(lib.icar_adv_set_stream(d.handle, C.c_void_p(st.cuda_stream)), d.handle)
+        for _ in range(5):
+            advect(d, opts, case.dt)
+        d.close()                       # five steps queued on the caller's stream
+        got = _run(case, 3)
+        for k in ref:
+            assert np.array_equal(got[k], ref[k]), k
+    st.synchronize()
